@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the lattice-Boltzmann hot path on B200.
+
+Workload (N=1 line): d3q27_cumulant, FP32, triply periodic Taylor-Green vortex
+on 256^3 nodes (u0=0.05, rho0=1, nu=1e-3), Globals every 50 iterations -- the
+configuration the MLUPS metric is quoted on. A *step* is one logging interval:
+49 plain iterations plus one iteration that integrates the Globals
+(ITER_LASTGLOB) and reads them back. ``value`` is MLUPS over K steps with the
+lattice resident in HBM; ``e2e`` is the same metric through the C ABI from
+host buffers: each e2e step uploads the initial snapshot from pinned host
+memory, runs the full 2000-iteration case with Globals every 50, and reads the
+velocity field back.
+
+Multi-GPU (torchrun, one rank per GPU): independent replicas, weak scaling, no
+data-path collective (the case does not shard across GPUs here).
+
+``--impl reference`` times the CPU restatement of the reference path (the
+oracle; TCLB itself cannot be built without R/polyAlgebra/MPI) on the host
+cores on a bounded slab of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS"
+UNIT = "MLUPS"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256, help="edge of the cubic lattice")
+    p.add_argument("--model", default="d3q27_cumulant")
+    p.add_argument("--precision", default="fp32")
+    p.add_argument("--storage", default="same")
+    p.add_argument("--log-every", type=int, default=50)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-iters", type=int, default=2000)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "of measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+def profiled_traffic(model, precision, storage, n):
+    """DRAM bytes per launch of the iteration kernel from the committed ncu
+    summary of this workload, if one exists (line 'traffic_bytes_per_launch: X'
+    under a heading naming the workload)."""
+    path = os.path.join(ROOT, "profiles", f"k_iterate_{model}_{precision}_{storage}_{n}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def tgv_setup(lat, n, u0=0.05, nu=1e-3):
+    from tclb_b200 import cases
+
+    lat.set_flags(cases.tgv_flags(lat.model, n, nz=lat.nz))
+    lat.SetSetting("nu", nu)
+    rho, u = cases.tgv_fields(n, u0=u0, nz=lat.nz, dtype=lat.real)
+    lat.init_equilibrium(rho, u)
+
+
+def cpu_baseline(args, model_name, seconds, threads=None):
+    """The oracle (CPU restatement of the reference path) on a slab of the
+    workload: 256 x 256 x cpu_slab nodes, periodic, same settings."""
+    import oracle
+    from tclb_b200 import cases
+    from tclb_b200 import models as M
+
+    cores = oracle.set_threads(threads or os.cpu_count() or 1)
+    n, nz = args.n, args.cpu_slab
+    o = oracle.OracleLattice(model_name, n, n, nz, precision=args.precision if args.precision == "fp64" else "fp32")
+    o.set_flags(cases.tgv_flags(model_name, n, nz=nz))
+    o.set_setting("nu", 1e-3)
+    m = M.get(model_name)
+    rho, u = cases.tgv_fields(n, u0=0.05, nz=nz, dtype=np.float64)
+    J = rho[..., None] * u
+    e = np.array(m.velocities, float)
+    w = np.array(m.weights)
+    eu = np.einsum("qd,zyxd->qzyx", e, J)
+    f = w[:, None, None, None] * (rho + 3 * eu + 4.5 * eu ** 2 / rho - 1.5 * (J ** 2).sum(-1) / rho)
+    o.set_densities(f)
+    del f, eu, J
+    o.iterate(1)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.iterate(1)
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and done >= 2:
+            break
+    mlups = n * n * nz * done / el / 1e6
+    return {"value": mlups, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{model_name} TGV slab {n}x{n}x{nz}, {done} iterations in {el:.1f} s, {args.precision}, "
+                      f"OpenMP over nodes (TCLB CPU build unavailable: needs R+polyAlgebra, autoconf, MPI)"}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    # each step a bounded sample (about cpu_seconds / 4 of CPU time)
+    per = max(1.0, args.cpu_seconds / 4)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_baseline(args, args.model, 0.5)
+    vals = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps if args.steps <= 5 else 5):
+        r = cpu_baseline(args, args.model, per)
+        vals.append(r["value"])
+    el = time.perf_counter() - t_all
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(vals),
+            "warmup": args.warmup, "ms_per_step": el / len(vals) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"{args.model} Taylor-Green {args.n}^3 sampled as {args.n}x{args.n}x{args.cpu_slab} "
+                                   f"slabs", "precision": args.precision, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            t = torch.ones(1, device="cuda")
+            dist.all_reduce(t)
+        torch.cuda.synchronize()
+
+    def reduce_max(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from tclb_b200 import models as M
+    from tclb_b200.lattice import Lattice
+
+    n, I = args.n, args.log_every
+    # CPU baseline first (rank 0, N=1): host-only work before the GPU is busy
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, args.model, args.cpu_seconds)
+
+    lat = Lattice(args.model, n, n, n, precision=args.precision, storage=args.storage)
+    tgv_setup(lat, n)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    N = lat.N
+    bpu = lat.bytes_per_update
+
+    for _ in range(args.warmup):
+        lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
+        lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+    barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    phys = vis.split(",")[local] if vis and len(vis.split(",")) > local else str(local)
+    clocks = ClockSampler(phys)
+    clocks.start()
+    time.sleep(0.3)
+    pairs = []
+    t_wall0 = time.perf_counter()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e_start.record(stream)
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
+        b.record(stream)
+        lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        pairs.append((a, b))
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    t = e_start.elapsed_time(e_end) / 1e3
+    t_max = reduce_max(t)
+    kern = sum(a.elapsed_time(b) for a, b in pairs) / 1e3 / (args.steps * (I - 1))
+    kern = reduce_max(kern)
+    glob = lat.globals_dict()
+    updates = N * I * args.steps
+    value = updates * world / t_max / 1e6
+
+    peaks, peak_src = measured_peaks()
+    achieved = bpu * N / kern / 1e9
+    traffic = profiled_traffic(args.model, args.precision, args.storage, n)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
+            "kernel": "k_iterate (no-Globals variant)", "bytes_per_update": bpu,
+            "kernel_ms": kern * 1e3, "kernel_mlups": N / kern / 1e6}
+
+    # ---- end to end through the C ABI from pinned host buffers -------------
+    e2e = None
+    if not args.no_e2e and args.e2e_steps > 0:
+        snap = torch.empty(lat.snapshot_bytes(), dtype=torch.uint8, pin_memory=True)
+        lat.save(snap.data_ptr(), stream=sp)
+        ubuf = torch.empty(N * 3, dtype=torch.float32 if args.precision == "fp32" else torch.float64,
+                           pin_memory=True)
+        uview = ubuf.numpy()
+        nlog = args.e2e_iters // I
+        gl_bytes = len(lat.model.globals) * 8
+        barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.e2e_steps):
+            lat.load(snap.data_ptr(), stream=sp)
+            for _ in range(nlog):
+                lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
+                lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+            lat.GetQuantity("U", out=uview, stream=sp)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        te = reduce_max(s0.elapsed_time(s1) / 1e3)
+        e2e = {"value": N * nlog * I * args.e2e_steps * world / te / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(snap.numel()),
+               "d2h_bytes_per_step": int(ubuf.numel() * ubuf.element_size() + nlog * gl_bytes),
+               "steps": args.e2e_steps, "iterations_per_step": nlog * I,
+               "step": "upload snapshot (pinned), full case with Globals every 50, read U back"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": f"{args.model} Taylor-Green vortex {n}^3 periodic, u0=0.05, nu=1e-3",
+                           "model": args.model, "lattice": [n, n, n], "precision": args.precision,
+                           "storage": args.storage, "iterations_per_step": I, "globals_every": I,
+                           "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % (bpu / 2 * N / 1e9),
+                           "parallelism": f"replicas x{world}"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": args.steps * I, "wall_s": wall,
+                "globals_last": {k: float(v) for k, v in glob.items()}}
+        print(json.dumps(line), flush=True)
+    lat.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,138 @@
+/*
+ * tclb_b200 -- C ABI of the B200 lattice-Boltzmann engine.
+ *
+ * Drop-in for the Run path of TCLB's `Lattice` class (src/Lattice.h.Rt:39-191)
+ * for the d2q9, d3q19 and d3q27_cumulant models. Every entry point returns a
+ * status (TCLB_OK = 0, negative on error) instead of exiting the process as
+ * TCLB's HANDLE_ERROR does (src/cross.cu:24-32); tclb_last_error() gives the
+ * message. Handles are independent, so many lattices may live in one process
+ * and on one GPU (TCLB keeps one lattice per process in __constant__ memory).
+ *
+ * Buffers passed in are host memory owned by the caller unless stated
+ * otherwise; pinned host memory makes the copies asynchronous-capable.
+ * `stream` arguments are cudaStream_t values passed as void* (NULL = the
+ * lattice's own stream).
+ */
+#ifndef TCLB_B200_H
+#define TCLB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tclb_lattice* tclb_h;
+
+/* models */
+#define TCLB_MODEL_D2Q9 0
+#define TCLB_MODEL_D3Q19 1
+#define TCLB_MODEL_D3Q27_CUMULANT 2
+
+/* arithmetic precision of the collision (real_t) */
+#define TCLB_FP32 0
+#define TCLB_FP64 1
+
+/* storage format of the densities (storage_t); *_SHIFT stores f_i - w_i */
+#define TCLB_STORAGE_SAME 0
+#define TCLB_STORAGE_FP16 1
+#define TCLB_STORAGE_FP16_SHIFT 2
+#define TCLB_STORAGE_BF16 3
+#define TCLB_STORAGE_BF16_SHIFT 4
+
+/* iteration flags, same values as src/Lattice.h.Rt:19-31 */
+#define TCLB_ITER_NORM 0x001
+#define TCLB_ITER_GLOBS 0x010
+#define TCLB_ITER_INTEG 0x070
+#define TCLB_ITER_LASTGLOB 0x080
+
+#define TCLB_OK 0
+#define TCLB_ERR_ARG (-1)
+#define TCLB_ERR_CUDA (-2)
+#define TCLB_ERR_MEMORY (-3)
+#define TCLB_ERR_STATE (-4)
+
+/* Message of the last failing call on this thread. */
+const char* tclb_last_error(void);
+
+/* Model description: number of densities Q, Settings, ZoneSettings, Globals,
+   Quantities, and the ZONE_SHIFT of the node-type word. Replaces the
+   R-generated constants of src/conf.R:859-891. */
+int tclb_model_info(int model, int* Q, int* nsettings, int* nzonesettings, int* nglobals, int* nquantities,
+                    int* zone_shift);
+/* Name of item `i` of kind 0 Setting, 1 ZoneSetting, 2 Global, 3 NodeType,
+   4 Quantity; for NodeType also its value and group mask. */
+int tclb_model_item(int model, int kind, int i, const char** name, int* value, int* mask);
+
+/* Lattice(lbRegion, MPIInfo, nSnaps) (src/Lattice.cu.Rt:87-151): allocate the
+   two snapshots, node types, zonal settings and Globals in one pooled device
+   allocation on the current device. nx is used as given (TCLB's Solver pads
+   it to a multiple of 32 before, src/Solver.cpp.Rt:273). Settings start at
+   their defaults (src/Solver.cpp.Rt:276-281, :393). */
+int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, int storage);
+int tclb_destroy(tclb_h h);
+int tclb_get_size(tclb_h h, int* nx, int* ny, int* nz);
+
+/* Lattice::FlagOverwrite (src/Lattice.cu.Rt:1040-1054): copy a box of node
+   types (TCLB bit layout, x fastest) at offset (dx,dy,dz). */
+int tclb_set_flags(tclb_h h, const uint16_t* flags, int dx, int dy, int dz, int nx, int ny, int nz);
+int tclb_get_flags(tclb_h h, uint16_t* flags);
+
+/* Lattice::SetSetting (src/Lattice.cu.Rt:1350-1358): set and follow the
+   derived-setting chain (e.g. d2q9 Viscosity -> RelaxationRate -> S2). */
+int tclb_set_setting(tclb_h h, int setting, double value);
+int tclb_get_setting(tclb_h h, int setting, double* value);
+/* ZoneSettings::set (src/ZoneSettings.h:58-77); zone = -1 sets every zone. */
+int tclb_set_zone_setting(tclb_h h, int zone_setting, int zone, double value);
+
+/* Lattice::Init (src/Lattice.cu.Rt:799-821): BaseInit stage (equilibrium
+   from settings), resets the iteration counter and the Globals. */
+int tclb_init(tclb_h h);
+
+/* Every node set to the model's equilibrium (SetEquilibrum of each model's
+   Dynamics.c.Rt) at density rho[n] and momentum rho[n]*u[3n..3n+2]; arrays
+   are real_t (float for TCLB_FP32, double for TCLB_FP64), x fastest. This is
+   the initial condition that TCLB can only inject through <LoadBinary>
+   (src/Handlers/acLoadBinary.cpp:5-23). Resets the iteration counter and the
+   Globals like tclb_init. */
+int tclb_init_equilibrium(tclb_h h, const void* rho, const void* u, void* stream);
+
+/* Lattice::Iterate (src/Lattice.cu.Rt:900-989) for ITER_NORM: `niter`
+   pull-stream+collide iterations. ITER_LASTGLOB integrates Globals on the last
+   iteration only and replaces the host Globals with them; ITER_INTEG
+   integrates on every iteration and adds them. */
+int tclb_iterate(tclb_h h, int niter, int iter_type, void* stream);
+
+/* Lattice::globals[] after calcGlobals (src/Lattice.cu.Rt:1279-1315), FP64, in
+   TCLB order: SUM globals, Objective, MAX globals. */
+int tclb_get_globals(tclb_h h, double* out);
+int tclb_clear_globals(tclb_h h);
+
+/* Lattice::GetQuantity (src/Lattice.cu.Rt:1184-1222): quantity `q` over the
+   region (x0,y0,z0,nx,ny,nz) times `scale`, in the lattice's real_t (float for
+   TCLB_FP32, double for TCLB_FP64); vector quantities are 3 values per node. */
+int tclb_get_quantity(tclb_h h, int q, const int region[6], void* out, double scale, void* stream);
+
+/* Get_/Set_<field> for all densities at once: SoA [q][z][y][x] as double. */
+int tclb_get_densities(tclb_h h, double* out);
+int tclb_set_densities(tclb_h h, const double* in);
+
+/* Raw snapshot of the current densities in storage format (Lattice::save /
+   load, src/Lattice.cu.Rt:642-769, without TCLB's margin split). */
+size_t tclb_snapshot_bytes(tclb_h h);
+int tclb_save(tclb_h h, void* host, size_t bytes, void* stream);
+int tclb_load(tclb_h h, const void* host, size_t bytes, void* stream);
+
+/* Iterations done since Init, and the bytes one iteration moves
+   (2*Q*sizeof(storage_t) + sizeof(flag_t) per node). */
+int tclb_get_iteration(tclb_h h, long long* iter);
+double tclb_bytes_per_update(tclb_h h);
+
+/* Synchronise the lattice's stream. */
+int tclb_sync(tclb_h h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

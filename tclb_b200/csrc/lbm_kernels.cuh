@@ -1,0 +1,866 @@
+// Device code of the B200 lattice-Boltzmann engine: storage policies, the
+// per-node physics of the d2q9, d3q19 and d3q27_cumulant models, and the
+// fused pull-stream + collide + Globals kernel.
+//
+// Layout: densities are SoA, one plane of N = nx*ny*nz values per population,
+// planes 256-byte aligned (stride in elements), node index x + nx*(y + ny*z).
+// Two snapshots are kept (A/B); an iteration pulls f_i(x) from A at x - e_i
+// with periodic wrap on every axis (TCLB's single-rank margins,
+// src/Global.cpp.Rt:61-82, src/Lattice.cu.Rt:439-456), runs the node update
+// and stores f_i(x) into B (src/LatticeAccess.inc.cpp.Rt:299-347).
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+#include "tclb_models.h"
+
+namespace tclb {
+
+// ---------------------------------------------------------------------------
+// Storage policies: storage_t <-> real_t (src/LatticeAccess.inc.cpp.Rt:14-35).
+// Shifted formats store (f - w_i) and add w_i back on load.
+// ---------------------------------------------------------------------------
+struct StoreF64 {
+  typedef double T;
+  static constexpr bool shifted = false;
+  template <class R>
+  __device__ __forceinline__ static R load(const T* p, R) { return (R)__ldg(p); }
+  template <class R>
+  __device__ __forceinline__ static void store(T* p, R v, R) { __stcs(p, (double)v); }
+  __host__ static T from_double(double v, double) { return v; }
+  __host__ static double to_double(T v, double) { return v; }
+};
+struct StoreF32 {
+  typedef float T;
+  static constexpr bool shifted = false;
+  template <class R>
+  __device__ __forceinline__ static R load(const T* p, R) { return (R)__ldg(p); }
+  template <class R>
+  __device__ __forceinline__ static void store(T* p, R v, R) { __stcs(p, (float)v); }
+  __host__ static T from_double(double v, double) { return (float)v; }
+  __host__ static double to_double(T v, double) { return v; }
+};
+template <bool SHIFT>
+struct StoreF16 {
+  typedef __half T;
+  static constexpr bool shifted = SHIFT;
+  template <class R>
+  __device__ __forceinline__ static R load(const T* p, R s) {
+    float v = __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p))));
+    return SHIFT ? (R)v + s : (R)v;
+  }
+  template <class R>
+  __device__ __forceinline__ static void store(T* p, R v, R s) {
+    __half h = __float2half_rn((float)(SHIFT ? v - s : v));
+    __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
+  }
+  __host__ static T from_double(double v, double s) { return __float2half_rn((float)(SHIFT ? v - s : v)); }
+  __host__ static double to_double(T v, double s) { return (double)__half2float(v) + (SHIFT ? s : 0.0); }
+};
+template <bool SHIFT>
+struct StoreBF16 {
+  typedef __nv_bfloat16 T;
+  static constexpr bool shifted = SHIFT;
+  template <class R>
+  __device__ __forceinline__ static R load(const T* p, R s) {
+    unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));
+    float v = __uint_as_float(((unsigned)u) << 16);
+    return SHIFT ? (R)v + s : (R)v;
+  }
+  template <class R>
+  __device__ __forceinline__ static void store(T* p, R v, R s) {
+    __nv_bfloat16 h = __float2bfloat16_rn((float)(SHIFT ? v - s : v));
+    __stcs(reinterpret_cast<unsigned short*>(p), *reinterpret_cast<unsigned short*>(&h));
+  }
+  __host__ static T from_double(double v, double s) { return __float2bfloat16_rn((float)(SHIFT ? v - s : v)); }
+  __host__ static double to_double(T v, double s) { return (double)__bfloat162float(v) + (SHIFT ? s : 0.0); }
+};
+
+// ---------------------------------------------------------------------------
+// Kernel arguments
+// ---------------------------------------------------------------------------
+template <class R, int NSET>
+struct Args {
+  const void* src;
+  void* dst;
+  size_t stride;  // elements between population planes
+  const flag_t* flags;
+  int nx, ny, nz;
+  const R* zone;  // [zones][NZS] zonal settings
+  double* glob;   // device Globals (FP64)
+  R s[NSET];      // settings
+};
+
+// AddTo<Global>(x) with TCLB's Objective rule: every AddTo of a SUM Global
+// also adds that Global's zonal <Global>InObj weight to Objective
+// (src/cuda.cu.Rt:114-119).
+template <int NSUM, int OBJ, int INOBJ, class R>
+__device__ __forceinline__ void add_glob(R* g, int i, R x, const R* zs) {
+  g[i] += x;
+  if (i < NSUM) g[OBJ] += zs[i + INOBJ];
+}
+
+// ---------------------------------------------------------------------------
+// d2q9 (models/flow/d2q9/Dynamics.c.Rt), plain variant (bc=FALSE)
+// ---------------------------------------------------------------------------
+struct D2Q9 {
+  static constexpr int Q = 9, DIM = 2, NSET = d2q9::NSET, NZS = d2q9::NZS, NG = d2q9::NG, NSUM = d2q9::NSUM,
+                       ZONE_SHIFT = d2q9::ZONE_SHIFT;
+  __host__ __device__ static constexpr int ex(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0); }
+  __host__ __device__ static constexpr int ey(int i) { return (i == 2 || i == 5 || i == 6) ? 1 : ((i == 4 || i == 7 || i == 8) ? -1 : 0); }
+  __host__ __device__ static constexpr int ez(int) { return 0; }
+  __host__ __device__ static constexpr int opp(int i) { return i == 0 ? 0 : (i <= 4 ? ((i + 1) % 4) + 1 : ((i - 3) % 4) + 5); }
+  __host__ __device__ static constexpr double w(int i) { return i == 0 ? 4.0 / 9.0 : (i <= 4 ? 1.0 / 9.0 : 1.0 / 36.0); }
+
+  template <class R>
+  __device__ __forceinline__ static void glob(R* g, int i, R x, const R* zs) {
+    add_glob<NSUM, d2q9::G_Objective, d2q9::IN_OBJ_OFFSET>(g, i, x, zs);
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void bounce(R (&f)[Q]) {
+    R t;
+    t = f[1]; f[1] = f[3]; f[3] = t;
+    t = f[2]; f[2] = f[4]; f[4] = t;
+    t = f[5]; f[5] = f[7]; f[7] = t;
+    t = f[6]; f[6] = f[8]; f[8] = t;
+  }
+
+  // ZouHeRewrite (lib/boundary.R:143-198) solved in closed form for the D2Q9
+  // second-order equilibrium. Outward normal n = SG*e_AX; unknowns have
+  // e.n < 0 and become f_opp + (feq_i - feq_opp)(R) = f_opp + 6 w_i e_i.R.
+  template <int AX, int SG, bool VEL, class R>
+  __device__ __forceinline__ static void zouhe(R (&f)[Q], R vx, R vy, R rho0) {
+    R S = 0, T = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+      const int ea = AX == 0 ? ex(i) : ey(i), et = AX == 0 ? ey(i) : ex(i);
+      if (ea == 0) { S += f[i]; T += (R)et * f[i]; }
+      else if (SG * ea > 0) S += R(2) * f[i];
+    }
+    R Rn, Rt;
+    if (VEL) {
+      const R vn = AX == 0 ? vx : vy, vt = AX == 0 ? vy : vx;
+      Rn = vn * S / (R(1) + R(SG) * vn);
+      const R rho = S - R(SG) * Rn;
+      Rt = R(3) * (vt * rho - T);
+    } else {
+      Rn = R(SG) * (S - rho0);
+      Rt = R(-3) * T;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+      const int ea = AX == 0 ? ex(i) : ey(i), et = AX == 0 ? ey(i) : ex(i);
+      if (SG * ea < 0) f[i] = f[opp(i)] + R(6.0 * w(i)) * (R(ea) * Rn + R(et) * Rt);
+    }
+  }
+
+  // Equilibrium / MRT moments in the Cholesky-weighted basis
+  // (d2q9/Dynamics.c.Rt:8-23): columns 1, x, y, 3x^2-1, 3y^2-1, 3xy,
+  // 3x^2y-y, 3xy^2-x, 9x^2y^2-3x^2-3y^2+1 with norms 1,1/3,1/3,2,2,1,2/3,2/3,4.
+  template <class R>
+  __device__ __forceinline__ static void from_moments(R (&f)[Q], R rho, R jx, R jy, R m3, R m4, R m5, R m6, R m7, R m8) {
+    const R r0 = rho, r1 = R(3) * jx, r2 = R(3) * jy, r3 = R(0.5) * m3, r4 = R(0.5) * m4, r5 = m5, r6 = R(1.5) * m6,
+            r7 = R(1.5) * m7, r8 = R(0.25) * m8;
+    const R a = r0 + R(2) * (r3 + r4) + R(4) * r8;
+    f[0] = R(4.0 / 9.0) * (r0 - r3 - r4 + r8);
+    f[1] = R(1.0 / 9.0) * (r0 + r1 + R(2) * r3 - r4 - r7 - R(2) * r8);
+    f[2] = R(1.0 / 9.0) * (r0 + r2 - r3 + R(2) * r4 - r6 - R(2) * r8);
+    f[3] = R(1.0 / 9.0) * (r0 - r1 + R(2) * r3 - r4 + r7 - R(2) * r8);
+    f[4] = R(1.0 / 9.0) * (r0 - r2 - r3 + R(2) * r4 + r6 - R(2) * r8);
+    f[5] = R(1.0 / 36.0) * (a + r1 + r2 + R(3) * r5 + R(2) * r6 + R(2) * r7);
+    f[6] = R(1.0 / 36.0) * (a - r1 + r2 - R(3) * r5 + R(2) * r6 - R(2) * r7);
+    f[7] = R(1.0 / 36.0) * (a - r1 - r2 + R(3) * r5 - R(2) * r6 - R(2) * r7);
+    f[8] = R(1.0 / 36.0) * (a + r1 - r2 - R(3) * r5 - R(2) * r6 + R(2) * r7);
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
+    const R d = f[5] + f[6] + f[7] + f[8];
+    const R rho = f[0] + f[1] + f[2] + f[3] + f[4] + d;
+    R jx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    R jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    R m3 = -f[0] + R(2) * (f[1] + f[3]) - f[2] - f[4] + R(2) * d;
+    R m4 = -f[0] - f[1] - f[3] + R(2) * (f[2] + f[4]) + R(2) * d;
+    R m5 = R(3) * (f[5] - f[6] + f[7] - f[8]);
+    R m6 = f[4] - f[2] + R(2) * (f[5] + f[6] - f[7] - f[8]);
+    R m7 = f[3] - f[1] + R(2) * (f[5] - f[6] - f[7] + f[8]);
+    R m8 = f[0] - R(2) * (f[1] + f[2] + f[3] + f[4]) + R(4) * d;
+    const R irho = R(1) / rho;
+    if (G) {  // d2q9/Dynamics.c.Rt:228-246 (pre-relaxation rho, J)
+      const unsigned obj = fl & d2q9::OBJECTIVE;
+      if (obj) {
+        const R usq = (jx * jx + jy * jy) / (rho * rho);
+        const R flux = jx / rho / rho;
+        const R pl = flux * ((rho - R(1)) / R(3) + usq / rho / R(2));
+        if (obj == d2q9::Outlet) { glob(g, d2q9::G_OutletFlux, flux, zs); glob(g, d2q9::G_PressureLoss, -pl, zs); }
+        else if (obj == d2q9::Inlet) { glob(g, d2q9::G_InletFlux, flux, zs); glob(g, d2q9::G_PressureLoss, pl, zs); }
+      }
+    }
+    const R S2 = a.s[d2q9::S_S2], S3 = a.s[d2q9::S_S3], S4 = a.s[d2q9::S_S4];
+    m3 = S2 * (m3 - R(3) * jx * jx * irho);
+    m4 = S2 * (m4 - R(3) * jy * jy * irho);
+    m5 = S2 * (m5 - R(3) * jx * jy * irho);
+    m6 = S3 * m6;
+    m7 = S3 * m7;
+    m8 = S4 * m8;
+    jx = jx + a.s[d2q9::S_GravitationX] * rho;
+    jy = jy + a.s[d2q9::S_GravitationY] * rho;
+    m3 += R(3) * jx * jx * irho;
+    m4 += R(3) * jy * jy * irho;
+    m5 += R(3) * jx * jy * irho;
+    from_moments(f, rho, jx, jy, m3, m4, m5, m6, m7, m8);
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void run(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g) {
+    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    const unsigned b = fl & d2q9::BOUNDARY;
+    if (b) {
+      const R vx = zs[d2q9::Z_VelocityX], vy = zs[d2q9::Z_VelocityY], rho0 = zs[d2q9::Z_Pressure] * R(3) + R(1);
+      switch (b) {  // d2q9/Dynamics.c.Rt:108-138
+        case d2q9::Solid:
+        case d2q9::Wall: bounce(f); break;
+        case d2q9::EVelocity: zouhe<0, 1, true>(f, vx, vy, rho0); break;
+        case d2q9::WPressure: zouhe<0, -1, false>(f, vx, vy, rho0); break;
+        case d2q9::WVelocity: zouhe<0, -1, true>(f, vx, vy, rho0); break;
+        case d2q9::EPressure: zouhe<0, 1, false>(f, vx, vy, rho0); break;
+        case d2q9::NVelocity: zouhe<1, 1, true>(f, vx, vy, rho0); break;
+        case d2q9::SVelocity: zouhe<1, -1, true>(f, vx, vy, rho0); break;
+        case d2q9::NSymmetry: f[4] = f[2]; f[7] = f[6]; f[8] = f[5]; break;  // Symmetry(2,-1)
+        case d2q9::SSymmetry: f[2] = f[4]; f[6] = f[7]; f[5] = f[8]; break;  // Symmetry(2, 1)
+        default: break;
+      }
+    }
+    if (fl & d2q9::MRT) mrt<R, G>(f, fl, a, g, zs);
+  }
+
+  // SetEquilibrum (:73-89): f = Req(rho, J) in the MRT basis, mapped back
+  template <class R>
+  __device__ __forceinline__ static void equilibrium(R (&f)[Q], R rho, R jx, R jy, R) {
+    const R irho = R(1) / rho;
+    from_moments(f, rho, jx, jy, R(3) * jx * jx * irho, R(3) * jy * jy * irho, R(3) * jx * jy * irho, R(0), R(0), R(0));
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void init(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, int, int, int) {
+    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    R rho = R(1) + zs[d2q9::Z_Pressure] * R(3), ux = zs[d2q9::Z_VelocityX], uy = zs[d2q9::Z_VelocityY];
+    if ((fl & d2q9::BOUNDARY) == d2q9::Wall) { rho = 1; ux = 0; uy = 0; }
+    equilibrium(f, rho, ux * rho, uy * rho, R(0));
+  }
+
+  // Quantities (d2q9/Dynamics.c.Rt:39-59): 0 Rho, 1 U
+  template <class R>
+  __device__ __forceinline__ static void quantity(int q, R (&f)[Q], flag_t, const Args<R, NSET>& a, R* out) {
+    R rho = 0, jx = 0, jy = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++) { rho += f[i]; jx += R(ex(i)) * f[i]; jy += R(ey(i)) * f[i]; }
+    if (q == 0) { out[0] = rho; return; }
+    out[0] = jx / rho + a.s[d2q9::S_GravitationX] * R(0.5);
+    out[1] = jy / rho + a.s[d2q9::S_GravitationY] * R(0.5);
+    out[2] = 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// d3q19 (models/flow/d3q19/Dynamics.c.Rt)
+// ---------------------------------------------------------------------------
+#include "d3q19_gen.cuh"
+
+struct D3Q19 {
+  static constexpr int Q = 19, DIM = 3, NSET = d3q19::NSET, NZS = d3q19::NZS, NG = d3q19::NG, NSUM = d3q19::NSUM,
+                       ZONE_SHIFT = d3q19::ZONE_SHIFT;
+  // directions: columns 4, 6, 8 of MRTMAT (d3q19/Dynamics.R:26-35)
+  __host__ __device__ static constexpr int ex(int i) {
+    return (i == 1 || i == 7 || i == 9 || i == 11 || i == 13) ? 1 : ((i == 2 || i == 8 || i == 10 || i == 12 || i == 14) ? -1 : 0);
+  }
+  __host__ __device__ static constexpr int ey(int i) {
+    return (i == 3 || i == 7 || i == 8 || i == 15 || i == 17) ? 1 : ((i == 4 || i == 9 || i == 10 || i == 16 || i == 18) ? -1 : 0);
+  }
+  __host__ __device__ static constexpr int ez(int i) {
+    return (i == 5 || i == 11 || i == 12 || i == 15 || i == 16) ? 1 : ((i == 6 || i == 13 || i == 14 || i == 17 || i == 18) ? -1 : 0);
+  }
+  __host__ __device__ static constexpr int opp(int i) {
+    return i == 0 ? 0 : (i <= 6 ? (i % 2 ? i + 1 : i - 1) : (i <= 10 ? 17 - i : (i <= 14 ? 25 - i : 33 - i)));
+  }
+  __host__ __device__ static constexpr double w(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
+
+  template <class R>
+  __device__ __forceinline__ static void glob(R* g, int i, R x, const R* zs) {
+    add_glob<NSUM, d3q19::G_Objective, d3q19::IN_OBJ_OFFSET>(g, i, x, zs);
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void bounce(R (&f)[Q]) {
+    R t;
+#pragma unroll
+    for (int i = 1; i < Q; i++)
+      if (opp(i) > i) { t = f[i]; f[i] = f[opp(i)]; f[opp(i)] = t; }
+  }
+  // sum f over directions with sign(e_x) == SX
+  template <int SX, class R>
+  __device__ __forceinline__ static R sumx(const R (&f)[Q]) {
+    R s = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++)
+      if ((ex(i) > 0 ? 1 : (ex(i) < 0 ? -1 : 0)) == SX) s += f[i];
+    return s;
+  }
+  template <class R>
+  __device__ __forceinline__ static void nxy(const R (&f)[Q], R& Nxy, R& Nxz) {
+    Nxy = (f[3] + f[15] + f[17] - f[4] - f[16] - f[18]) / R(2);
+    Nxz = (f[5] + f[15] + f[16] - f[6] - f[17] - f[18]) / R(2);
+  }
+  template <class R>
+  __device__ __forceinline__ static void inlet(R (&f)[Q], R rho, R ux) {  // :98-108
+    R Nxy, Nxz;
+    nxy(f, Nxy, Nxz);
+    f[1] = f[2] + rho * ux / R(3);
+    f[9] = f[8] + rho * ux / R(6) + Nxy;
+    f[7] = f[10] + rho * ux / R(6) - Nxy;
+    f[11] = f[14] + rho * ux / R(6) - Nxz;
+    f[13] = f[12] + rho * ux / R(6) + Nxz;
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
+    R m[Q];
+    d3q19_moments(f, m);
+    const R omega = a.s[d3q19::S_omega];
+    const R g1 = R(1) - omega;
+    const R g2 = R(1) - R(8) * (R(2) - omega) / (R(8) - omega);
+    const R rho = m[0], irho = R(1) / rho;
+    R jx = m[3], jy = m[5], jz = m[7];
+    // equilibrium moments of TCLB's d3q19 (lib/d3q19.R:40-62), 0-based index
+    auto req = [&](R Jx, R Jy, R Jz, R (&q)[Q]) {
+      const R j2 = (Jx * Jx + Jy * Jy + Jz * Jz) * irho;
+      const R pxx = (R(2) * Jx * Jx - Jy * Jy - Jz * Jz) * irho;
+      const R pww = (Jy * Jy - Jz * Jz) * irho;
+      q[1] = R(-11) * rho + R(19) * j2;
+      q[2] = R(3) * rho - R(2) * j2;
+      q[4] = R(-2.0 / 3.0) * Jx;
+      q[6] = R(-2.0 / 3.0) * Jy;
+      q[8] = R(-2.0 / 3.0) * Jz;
+      q[9] = pxx;
+      q[10] = -pxx;
+      q[11] = pww;
+      q[12] = -pww;
+      q[13] = Jx * Jy * irho;
+      q[14] = Jy * Jz * irho;
+      q[15] = Jx * Jz * irho;
+      q[16] = 0; q[17] = 0; q[18] = 0;
+    };
+    R q[Q];
+    req(jx, jy, jz, q);
+#pragma unroll
+    for (int k = 0; k < Q; k++) {
+      if (k == 0 || k == 3 || k == 5 || k == 7) continue;
+      const R s = (k == 1 || k == 2 || (k >= 9 && k <= 15)) ? g1 : g2;
+      m[k] = s * (m[k] - q[k]);
+    }
+    jx += rho * a.s[d3q19::S_ForceX];
+    jy += rho * a.s[d3q19::S_ForceY];
+    jz += rho * a.s[d3q19::S_ForceZ];
+    req(jx, jy, jz, q);
+#pragma unroll
+    for (int k = 0; k < Q; k++) {
+      if (k == 0 || k == 3 || k == 5 || k == 7) continue;
+      m[k] += q[k];
+    }
+    m[3] = jx; m[5] = jy; m[7] = jz;
+    const double mw[Q] = D3Q19_MW;
+#pragma unroll
+    for (int k = 0; k < Q; k++) m[k] *= R(1.0 / mw[k]);
+    d3q19_populations(m, f);
+    if (G) {  // :266-289, with rho and J already divided by Mw (C(R, Mw, eq="/="))
+      const R rs = m[0], ux = m[3] / rs, uy = m[5] / rs, uz = m[7] / rs;
+      const unsigned pl = fl & d3q19::ADDITIONALS;
+      if (pl) {
+        const int b = 1 + 5 * (int)(pl - 1);
+        glob(g, b + 0, ux, zs);
+        glob(g, b + 1, uy, zs);
+        glob(g, b + 2, uz, zs);
+        glob(g, b + 3, rs, zs);
+        glob(g, b + 4, R(1), zs);
+      }
+      glob(g, d3q19::G_VOLvx, ux, zs);
+      glob(g, d3q19::G_VOLvy, uy, zs);
+      glob(g, d3q19::G_VOLvz, uz, zs);
+      glob(g, d3q19::G_VOLpx, m[3], zs);
+      glob(g, d3q19::G_VOLpy, m[5], zs);
+      glob(g, d3q19::G_VOLpz, m[7], zs);
+      glob(g, d3q19::G_VOLrho, rs, zs);
+      glob(g, d3q19::G_VOLvolume, R(1), zs);
+      const R v = sqrt(ux * ux + uy * uy + uz * uz);
+      g[d3q19::G_MaxV] = g[d3q19::G_MaxV] > v ? g[d3q19::G_MaxV] : v;
+    }
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void run(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g) {
+    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    const unsigned b = fl & d3q19::BOUNDARY;
+    if (b) {
+      switch (b) {  // :181-204
+        case d3q19::WPressureL: {  // :138-153
+          R SF = sumx<-1>(f);
+          SF = sumx<0>(f) + R(2) * SF;
+          R rho = a.s[d3q19::S_InletDensity];
+          R ux = R(1) - SF / rho;
+          if (ux > a.s[d3q19::S_InletVelocity]) { ux = a.s[d3q19::S_InletVelocity]; rho = SF / (R(1) - ux); }
+          inlet(f, rho, ux);
+          break;
+        }
+        case d3q19::WPressure: {  // :124-136
+          const R rho = a.s[d3q19::S_InletDensity];
+          R ux = sumx<-1>(f);
+          ux = sumx<0>(f) + R(2) * ux;
+          ux = R(1) - ux / rho;
+          inlet(f, rho, ux);
+          break;
+        }
+        case d3q19::WVelocity: {  // :110-122
+          const R ux = a.s[d3q19::S_InletVelocity];
+          R rho = sumx<-1>(f);
+          rho = sumx<0>(f) + R(2) * rho;
+          rho = rho / (R(1) - ux);
+          inlet(f, rho, ux);
+          break;
+        }
+        case d3q19::EPressure: {  // :157-179
+          const R rho = 1;
+          R ux = sumx<1>(f);
+          ux = sumx<0>(f) + R(2) * ux;
+          ux = R(-1) + ux / rho;
+          R Nxy, Nxz;
+          nxy(f, Nxy, Nxz);
+          f[2] = f[1] - rho * ux / R(3);
+          f[8] = f[9] - rho * ux / R(6) - Nxy;
+          f[10] = f[7] - rho * ux / R(6) + Nxy;
+          f[14] = f[11] - rho * ux / R(6) + Nxz;
+          f[12] = f[13] - rho * ux / R(6) - Nxz;
+          break;
+        }
+        case d3q19::Wall:
+        case d3q19::Solid: bounce(f); break;
+        default: break;
+      }
+    }
+    if ((fl & d3q19::COLLISION) == d3q19::MRT) mrt<R, G>(f, fl, a, g, zs);
+  }
+
+  // SetEquilibrum (:212-217): f = Req(rho, J) . MRTMAT.inv
+  template <class R>
+  __device__ __forceinline__ static void equilibrium(R (&f)[Q], R rho, R jx, R jy, R jz) {
+    const R irho = R(1) / rho;
+    const R j2 = (jx * jx + jy * jy + jz * jz) * irho;
+    const R pxx = (R(2) * jx * jx - jy * jy - jz * jz) * irho;
+    const R pww = (jy * jy - jz * jz) * irho;
+    R m[Q];
+    m[0] = rho; m[1] = R(-11) * rho + R(19) * j2; m[2] = R(3) * rho - R(2) * j2;
+    m[3] = jx; m[4] = R(-2.0 / 3.0) * jx; m[5] = jy; m[6] = R(-2.0 / 3.0) * jy; m[7] = jz; m[8] = R(-2.0 / 3.0) * jz;
+    m[9] = pxx; m[10] = -pxx; m[11] = pww; m[12] = -pww;
+    m[13] = jx * jy * irho; m[14] = jy * jz * irho; m[15] = jx * jz * irho;
+    m[16] = 0; m[17] = 0; m[18] = 0;
+    const double mw[Q] = D3Q19_MW;
+#pragma unroll
+    for (int k = 0; k < Q; k++) m[k] *= R(1.0 / mw[k]);
+    d3q19_populations(m, f);
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void init(R (&f)[Q], flag_t, const Args<R, NSET>& a, int, int, int) {
+    // SetEquilibrum(1, InletVelocity, 0, 0) (:219-221)
+    equilibrium(f, R(1), a.s[d3q19::S_InletVelocity], R(0), R(0));
+  }
+
+  // Quantities (:23-40): 0 P, 1 U
+  template <class R>
+  __device__ __forceinline__ static void quantity(int q, R (&f)[Q], flag_t fl, const Args<R, NSET>&, R* out) {
+    R rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++) { rho += f[i]; jx += R(ex(i)) * f[i]; jy += R(ey(i)) * f[i]; jz += R(ez(i)) * f[i]; }
+    if (q == 0) { out[0] = (rho - R(1)) / R(3); return; }
+    if ((fl & d3q19::BOUNDARY) == d3q19::Wall) { out[0] = out[1] = out[2] = 0; return; }
+    out[0] = jx / rho; out[1] = jy / rho; out[2] = jz / rho;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// d3q27_cumulant (models/flow/d3q27_cumulant/Dynamics.c.Rt), plain variant
+// ---------------------------------------------------------------------------
+#include "cumulant_gen.cuh"
+
+struct D3Q27C {
+  static constexpr int Q = 27, DIM = 3, NSET = d3q27c::NSET, NZS = d3q27c::NZS, NG = d3q27c::NG,
+                       NSUM = d3q27c::NSUM, ZONE_SHIFT = d3q27c::ZONE_SHIFT;
+  // f<a><b><c>: index a + 3b + 9c, digit 0 -> 0, 1 -> +1, 2 -> -1
+  __host__ __device__ static constexpr int dg(int v) { return v == 1 ? 1 : (v == 2 ? -1 : 0); }
+  __host__ __device__ static constexpr int ex(int i) { return dg(i % 3); }
+  __host__ __device__ static constexpr int ey(int i) { return dg((i / 3) % 3); }
+  __host__ __device__ static constexpr int ez(int i) { return dg(i / 9); }
+  __host__ __device__ static constexpr int od(int v) { return (3 - v) % 3; }
+  __host__ __device__ static constexpr int opp(int i) { return od(i % 3) + 3 * od((i / 3) % 3) + 9 * od(i / 9); }
+  __host__ __device__ static constexpr int mirror_y(int i) { return i % 3 + 3 * od((i / 3) % 3) + 9 * (i / 9); }
+  __host__ __device__ static constexpr int nnz(int i) { return (i % 3 != 0) + ((i / 3) % 3 != 0) + (i / 9 != 0); }
+  __host__ __device__ static constexpr double w(int i) {
+    return nnz(i) == 0 ? 8.0 / 27.0 : (nnz(i) == 1 ? 2.0 / 27.0 : (nnz(i) == 2 ? 1.0 / 54.0 : 1.0 / 216.0));
+  }
+  __host__ __device__ static constexpr int ea(int i, int ax) { return ax == 0 ? ex(i) : (ax == 1 ? ey(i) : ez(i)); }
+
+  template <class R>
+  __device__ __forceinline__ static void glob(R* g, int i, R x, const R* zs) {
+    add_glob<NSUM, d3q27c::G_Objective, d3q27c::IN_OBJ_OFFSET>(g, i, x, zs);
+  }
+
+  // ZouHe (lib/boundary.R:67-108) in closed form: unknowns SG*e_AX > 0 become
+  // f_opp + 6 w_i e_i.J; rho/J_AX from the density equation, tangential J
+  // from zero tangential momentum.
+  template <int AX, int SG, bool VEL, class R>
+  __device__ __forceinline__ static void zouhe(R (&f)[Q], R P, R V) {
+    R S = 0, T1 = 0, T2 = 0;
+    constexpr int A1 = (AX + 1) % 3, A2 = (AX + 2) % 3;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+      const int e = ea(i, AX);
+      if (e == 0) { S += f[i]; T1 += R(ea(i, A1)) * f[i]; T2 += R(ea(i, A2)) * f[i]; }
+      else if (SG * e < 0) S += R(2) * f[i];
+    }
+    R J[3];
+    if (VEL) {
+      const R rho = S / (R(1) - R(SG) * V);
+      J[AX] = rho * V;
+    } else {
+      const R rho = P * R(3) + R(1);
+      J[AX] = R(SG) * (rho - S);
+    }
+    J[A1] = R(-3) * T1;
+    J[A2] = R(-3) * T2;
+#pragma unroll
+    for (int i = 0; i < Q; i++)
+      if (SG * ea(i, AX) > 0)
+        f[i] = f[opp(i)] + R(6.0 * w(i)) * (R(ex(i)) * J[0] + R(ey(i)) * J[1] + R(ez(i)) * J[2]);
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void bounce_drag(R (&f)[Q], flag_t fl, R* g, const R* zs) {
+    R p1x = 0, p1y = 0, p1z = 0, p2x = 0, p2y = 0, p2z = 0;
+    if (G) {
+#pragma unroll
+      for (int i = 0; i < Q; i++) { p1x += R(ex(i)) * f[i]; p1y += R(ey(i)) * f[i]; p1z += R(ez(i)) * f[i]; }
+    }
+#pragma unroll
+    for (int i = 1; i < Q; i++)
+      if (opp(i) > i) { const R t = f[i]; f[i] = f[opp(i)]; f[opp(i)] = t; }
+    if (G && (fl & d3q27c::BODY) == d3q27c::Body) {  // :121-126
+#pragma unroll
+      for (int i = 0; i < Q; i++) { p2x += R(ex(i)) * f[i]; p2y += R(ey(i)) * f[i]; p2z += R(ez(i)) * f[i]; }
+      glob(g, d3q27c::G_Drag, -(p2x - p1x), zs);
+      glob(g, d3q27c::G_Lateral, -(p2y - p1y), zs);
+      glob(g, d3q27c::G_Lift, -(p2z - p1z), zs);
+    }
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void boundaries(R (&f)[Q], flag_t fl, R* g, const R* zs) {  // :224-272
+    const unsigned ad = fl & d3q27c::ADDITIONALS;
+    if (ad == d3q27c::NSymmetry) {
+#pragma unroll
+      for (int i = 0; i < Q; i++) if (ey(i) < 0) f[i] = f[mirror_y(i)];
+    } else if (ad == d3q27c::SSymmetry) {
+#pragma unroll
+      for (int i = 0; i < Q; i++) if (ey(i) > 0) f[i] = f[mirror_y(i)];
+    }
+    const unsigned b = fl & d3q27c::BOUNDARY;
+    if (!b) return;
+    const R V = zs[d3q27c::Z_Velocity], P = zs[d3q27c::Z_Pressure];
+    switch (b) {
+      case d3q27c::WVelocityTurbulent: zouhe<0, 1, true>(f, P, V); break;  // zero turbulence intensity
+      case d3q27c::EPressure: zouhe<0, -1, false>(f, P, V); break;
+      case d3q27c::WPressure: zouhe<0, 1, false>(f, P, V); break;
+      case d3q27c::SPressure: zouhe<1, 1, false>(f, P, V); break;
+      case d3q27c::NPressure: zouhe<1, -1, false>(f, P, V); break;
+      case d3q27c::WVelocity: zouhe<0, 1, true>(f, P, V); break;
+      case d3q27c::NVelocity: zouhe<1, -1, true>(f, P, V); break;
+      case d3q27c::SVelocity: zouhe<1, 1, true>(f, P, V); break;
+      case d3q27c::EVelocity: zouhe<0, -1, true>(f, P, V); break;
+      case d3q27c::Wall: bounce_drag<R, G>(f, fl, g, zs); break;
+      default: break;
+    }
+  }
+
+  // 1D raw-moment transform of a (0, +1, -1) triple and its inverse
+  // (:323-349 and :479-505)
+  template <class R>
+  __device__ __forceinline__ static void raw3(R& a0, R& a1, R& a2) {
+    a0 = a2 + a1 + a0;
+    a1 = a1 - a2;
+    a2 = a1 + a2 * R(2);
+  }
+  template <class R>
+  __device__ __forceinline__ static void unraw3(R& a0, R& a1, R& a2) {
+    a0 = a0 - a2;
+    a1 = (a2 + a1) * R(0.5);
+    a2 = a2 - a1;
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void collide(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
+    const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
+    if (G) {  // :311-319, getU_ :30-45
+      R rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+      for (int i = 0; i < Q; i++) { rho += f[i]; jx += R(ex(i)) * f[i]; jy += R(ey(i)) * f[i]; jz += R(ez(i)) * f[i]; }
+      R ux = (jx + Fx / R(2)) / rho, uy = (jy + Fy / R(2)) / rho, uz = (jz + Fz / R(2)) / rho;
+      if ((fl & d3q27c::BOUNDARY) == d3q27c::Wall) ux = uy = uz = 0;
+      glob(g, d3q27c::G_Density, rho, zs);
+      glob(g, d3q27c::G_Flux, ux, zs);
+      glob(g, d3q27c::G_Mass, rho, zs);
+      glob(g, d3q27c::G_XMomentum, rho * ux, zs);
+      glob(g, d3q27c::G_YMomentum, rho * uy, zs);
+      glob(g, d3q27c::G_ZMomentum, rho * uz, zs);
+    }
+    const R w0 = (fl & d3q27c::BOUNDARY) ? R(1) / (R(3) * a.s[d3q27c::S_nubuffer] + R(0.5))
+                                         : R(1) / (R(3) * a.s[d3q27c::S_nu] + R(0.5));
+    const R w1 = R(1);
+    // raw moments: x, y, z passes
+#pragma unroll
+    for (int r = 0; r < 27; r += 3) raw3(f[r], f[r + 1], f[r + 2]);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) raw3(f[x + 9 * c], f[x + 3 + 9 * c], f[x + 6 + 9 * c]);
+#pragma unroll
+    for (int r = 0; r < 9; r++) raw3(f[r], f[r + 9], f[r + 18]);
+    R c[Q];
+    const R m0 = f[0], im0 = R(1) / m0;
+    cum_from_raw(f, c, im0);
+    // relaxation (:386-449)
+    const R ux = c[1] + Fx * R(0.5) * im0, uy = c[3] + Fy * R(0.5) * im0, uz = c[9] + Fz * R(0.5) * im0;
+    const R c200 = c[2], c020 = c[6], c002 = c[18];
+    const R dxu = -w0 / R(2) * (R(2) * c200 - c020 - c002) - w1 / R(2) * (c200 + c020 + c002 - R(1));
+    const R dyv = dxu + R(3) * w0 / R(2) * (c200 - c020);
+    const R dzw = dxu + R(3) * w0 / R(2) * (c200 - c002);
+    const R gcor1 = R(3) * (R(1) - w0 / R(2)) * (ux * ux * dxu - uy * uy * dyv);
+    const R gcor2 = R(3) * (R(1) - w0 / R(2)) * (ux * ux * dxu - uz * uz * dzw);
+    const R gcor3 = R(3) * (R(1) - w1 / R(2)) * (ux * ux * dxu + uy * uy * dyv + uz * uz * dzw);
+    const R GC = a.s[d3q27c::S_GalileanCorrection];
+    const R A = (R(1) - w0) * (c200 - c020) - gcor1 * GC;
+    const R B = (R(1) - w0) * (c200 - c002) - gcor2 * GC;
+    const R CC = w1 + (R(1) - w1) * (c200 + c020 + c002) - gcor3 * GC;
+    c[1] += Fx;
+    c[2] = (A + B + CC) / R(3);
+    c[6] = (CC - R(2) * A + B) / R(3);
+    c[18] = (CC - R(2) * B + A) / R(3);
+    c[3] += Fy;
+    c[9] += Fz;
+    c[4] *= (R(1) - w0);
+    c[12] *= (R(1) - w0);
+    c[10] *= (R(1) - w0);
+    const R om3 = R(1) - a.s[d3q27c::S_Omega];
+#pragma unroll
+    for (int n = 1; n < Q; n++) {
+      const int s = n % 3 + (n / 3) % 3 + n / 9;
+      if (s == 3) c[n] = om3 * c[n];
+      if (s > 3) c[n] = 0;
+    }
+    raw_from_cum(c, f, m0);
+    // back to populations: x, y, z passes
+#pragma unroll
+    for (int r = 0; r < 27; r += 3) unraw3(f[r], f[r + 1], f[r + 2]);
+#pragma unroll
+    for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) unraw3(f[x + 9 * cc], f[x + 3 + 9 * cc], f[x + 6 + 9 * cc]);
+#pragma unroll
+    for (int r = 0; r < 9; r++) unraw3(f[r], f[r + 9], f[r + 18]);
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void run(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g) {
+    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    if (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) boundaries<R, G>(f, fl, g, zs);
+    if ((fl & d3q27c::COLLISION) == d3q27c::MRT) collide<R, G>(f, fl, a, g, zs);
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void equilibrium(R (&f)[Q], R rho, R jx, R jy, R jz) {
+    const R irho = R(1) / rho, j2 = (jx * jx + jy * jy + jz * jz) * irho;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+      const R eu = R(ex(i)) * jx + R(ey(i)) * jy + R(ez(i)) * jz;
+      f[i] = R(w(i)) * (rho + R(3) * eu + R(4.5) * eu * eu * irho - R(1.5) * j2);
+    }
+  }
+
+  template <class R>
+  __device__ __forceinline__ static void init(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, int, int, int) {
+    // :290-299 with zero synthetic turbulence: SetEquilibrum(1+3P, Velocity, 0, 0)
+    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    if ((fl & d3q27c::BOUNDARY) == d3q27c::Wall) equilibrium(f, R(1), R(0), R(0), R(0));
+    else equilibrium(f, R(1) + zs[d3q27c::Z_Pressure] * R(3), zs[d3q27c::Z_Velocity], R(0), R(0));
+  }
+
+  // Quantities (:23-60): 0 P, 1 U (after RunBoundaries), 2 Solid
+  template <class R>
+  __device__ __forceinline__ static void quantity(int q, R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* out) {
+    const bool wall = (fl & d3q27c::BOUNDARY) == d3q27c::Wall;
+    if (q == 2) { out[0] = wall ? R(1) : R(0); return; }
+    if (q == 1) {
+      const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+      boundaries<R, false>(f, fl, nullptr, zs);
+    }
+    R rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++) { rho += f[i]; jx += R(ex(i)) * f[i]; jy += R(ey(i)) * f[i]; jz += R(ez(i)) * f[i]; }
+    if (q == 0) { out[0] = (rho - R(1)) / R(3); return; }
+    if (wall) { out[0] = out[1] = out[2] = 0; return; }
+    out[0] = (jx + a.s[d3q27c::S_ForceX] / R(2)) / rho;
+    out[1] = (jy + a.s[d3q27c::S_ForceY] / R(2)) / rho;
+    out[2] = (jz + a.s[d3q27c::S_ForceZ] / R(2)) / rho;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Globals: warp shuffle -> shared memory -> one FP64 atomic per Global per
+// block (replaces CudaAtomicAddReduceWarp / MaxReduceWarp, src/cross.hpp:163-181).
+// MAX Globals are non-negative here, so an integer max on the FP64 bits orders
+// them correctly.
+// ---------------------------------------------------------------------------
+template <int NG, int NSUM, class R>
+__device__ __forceinline__ void reduce_globals(const R (&g)[NG], double* out) {
+  __shared__ double sh[32][NG];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NG; i++) {
+    double v = (double)g[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_down_sync(0xffffffffu, v, o);
+      v = i < NSUM ? v + u : (u > v ? u : v);
+    }
+    if (lane == 0) sh[warp][i] = v;
+  }
+  __syncthreads();
+  if (tid < NG) {
+    double v = sh[0][tid];
+    for (int w = 1; w < nwarps; w++) v = tid < NSUM ? v + sh[w][tid] : (sh[w][tid] > v ? sh[w][tid] : v);
+    if (tid < NSUM) {
+      if (v != 0.0) atomicAdd(out + tid, v);
+    } else if (v > 0.0) {
+      atomicMax(reinterpret_cast<unsigned long long*>(out + tid), (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The fused iteration kernel: one thread per node.
+// ---------------------------------------------------------------------------
+template <class M, class R, class St, bool G>
+__global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool act = (x < a.nx) && (y < a.ny);
+  R g[M::NG];
+  if (G) {
+#pragma unroll
+    for (int i = 0; i < M::NG; i++) g[i] = 0;
+  }
+  if (act) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
+    const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
+    const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
+    const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src);
+    typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst);
+    const int node = x + nx * (y + ny * z);
+    const flag_t fl = a.flags[node];
+    R f[M::Q];
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const int sx = M::ex(i) == 0 ? x : (M::ex(i) > 0 ? xm : xp);
+      const int sy = M::ey(i) == 0 ? y : (M::ey(i) > 0 ? ym : yp);
+      const int sz = M::DIM == 2 ? z : (M::ez(i) == 0 ? z : (M::ez(i) > 0 ? zm : zp));
+      f[i] = St::template load<R>(src + (size_t)i * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(i)));
+    }
+    M::template run<R, G>(f, fl, a, g);
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
+  }
+  if (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+}
+
+// BaseInit stage: equilibrium from settings, written to the current snapshot.
+template <class M, class R, class St>
+__global__ void k_init(const Args<R, M::NSET> a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= a.nx || y >= a.ny) return;
+  const int node = x + a.nx * (y + a.ny * z);
+  R f[M::Q];
+  M::template init<R>(f, a.flags[node], a, x, y, z);
+  typename St::T* dst = static_cast<typename St::T*>(a.dst);
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
+}
+
+// Equilibrium from density and velocity fields (J = rho u), the initial
+// condition of cases that TCLB loads through <LoadBinary>.
+template <class M, class R, class St>
+__global__ void k_equilibrium(const Args<R, M::NSET> a, const R* __restrict__ rho, const R* __restrict__ u) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= a.nx || y >= a.ny) return;
+  const int node = x + a.nx * (y + a.ny * z);
+  const R r = rho[node];
+  R f[M::Q];
+  M::template equilibrium<R>(f, r, r * u[3 * (size_t)node], r * u[3 * (size_t)node + 1], r * u[3 * (size_t)node + 2]);
+  typename St::T* dst = static_cast<typename St::T*>(a.dst);
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
+}
+
+// Quantity over a region (LatticeContainer.inc.cpp.Rt:437-473): pull, then
+// the model's get<Q>(), times scale. Region origin (rx,ry,rz), size (rnx,rny).
+template <class M, class R, class St>
+__global__ void k_quantity(const Args<R, M::NSET> a, int q, int vec, int rx, int ry, int rz, int rnx, int rny,
+                           int rnz, R scale, R* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= rnx || j >= rny || k >= rnz) return;
+  const int x = rx + i, y = ry + j, z = rz + k;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
+  const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
+  const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
+  const typename St::T* src = static_cast<const typename St::T*>(a.src);
+  R f[M::Q];
+#pragma unroll
+  for (int d = 0; d < M::Q; d++) {
+    const int sx = M::ex(d) == 0 ? x : (M::ex(d) > 0 ? xm : xp);
+    const int sy = M::ey(d) == 0 ? y : (M::ey(d) > 0 ? ym : yp);
+    const int sz = M::DIM == 2 ? z : (M::ez(d) == 0 ? z : (M::ez(d) > 0 ? zm : zp));
+    f[d] = St::template load<R>(src + (size_t)d * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(d)));
+  }
+  R v[3];
+  M::template quantity<R>(q, f, a.flags[x + nx * (y + ny * z)], a, v);
+  const size_t o = (size_t)i + (size_t)rnx * ((size_t)j + (size_t)rny * k);
+  if (vec) {
+    out[3 * o] = v[0] * scale;
+    out[3 * o + 1] = v[1] * scale;
+    out[3 * o + 2] = v[2] * scale;
+  } else {
+    out[o] = v[0] * scale;
+  }
+}
+
+}  // namespace tclb

@@ -1,0 +1,636 @@
+// Host runtime and C ABI of the B200 lattice-Boltzmann engine.
+//
+// One handle = one lattice (TCLB's Lattice + LatticeContainer, src/Lattice.cu.Rt,
+// src/LatticeContainer.h.Rt): a single pooled device allocation holds both
+// snapshots, the node types, the zonal-settings table and the FP64 Globals
+// (TCLB pools its buffers the same way, src/cross.cu:52-102). Settings travel
+// as kernel parameters instead of __constant__ memory, so handles are
+// independent and any number of lattices can share a GPU.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tclb_b200.h"
+#include "lbm_kernels.cuh"
+
+using namespace tclb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define TCLB_CK(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(TCLB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ model tables
+const double NA = NAN;
+
+const char* const d2q9_set[] = {"RelaxationRate", "Viscosity", "GravitationX", "GravitationY", "S2", "S3", "S4",
+                                "Threshold"};
+const double d2q9_set_def[] = {NA, NA, 0, 0, 0, 0, 0, 0.5};
+const int d2q9_set_der[] = {d2q9::S_S2, d2q9::S_RelaxationRate, -1, -1, -1, -1, -1, -1};
+const char* const d2q9_zs[] = {"VelocityX", "VelocityY", "Pressure", "PressureLossInObj", "OutletFluxInObj",
+                               "InletFluxInObj"};
+const double d2q9_zs_def[] = {0, 0, 0, 0, 0, 0};
+const char* const d2q9_gl[] = {"PressureLoss", "OutletFlux", "InletFlux", "Objective"};
+const char* const d2q9_nt[] = {"EPressure", "WPressure", "NVelocity", "SVelocity", "WVelocity", "EVelocity", "NSymmetry",
+                               "SSymmetry", "Solid", "Wall", "MRT", "Inlet", "Outlet"};
+const int d2q9_nt_v[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 0x10, 0x20, 0x40};
+const int d2q9_nt_m[] = {0xF, 0xF, 0xF, 0xF, 0xF, 0xF, 0xF, 0xF, 0xF, 0xF, 0x10, 0x60, 0x60};
+const char* const d2q9_q[] = {"Rho", "U"};
+const int d2q9_qv[] = {0, 1};
+
+const char* const d3q19_set[] = {"omega", "nu", "InletVelocity", "InletPressure", "InletDensity", "ForceX", "ForceY",
+                                 "ForceZ", "Threshold"};
+const double d3q19_set_def[] = {0, NA, 0, NA, 1, 0, 0, 0, 0.5};
+const int d3q19_set_der[] = {-1, d3q19::S_omega, -1, d3q19::S_InletDensity, -1, -1, -1, -1, -1};
+const char* const d3q19_gl[] = {"Flux",   "XYvx",   "XYvy",   "XYvz",   "XYrho",     "XYarea",    "XZvx",
+                                "XZvy",   "XZvz",   "XZrho",  "XZarea", "YZvx",      "YZvy",      "YZvz",
+                                "YZrho",  "YZarea", "VOLvx",  "VOLvy",  "VOLvz",     "VOLpx",     "VOLpy",
+                                "VOLpz",  "VOLrho", "VOLvolume", "Objective", "MaxV"};
+const char* const d3q19_zs[] = {"FluxInObj",   "XYvxInObj",   "XYvyInObj",  "XYvzInObj",   "XYrhoInObj",
+                                "XYareaInObj", "XZvxInObj",   "XZvyInObj",  "XZvzInObj",   "XZrhoInObj",
+                                "XZareaInObj", "YZvxInObj",   "YZvyInObj",  "YZvzInObj",   "YZrhoInObj",
+                                "YZareaInObj", "VOLvxInObj",  "VOLvyInObj", "VOLvzInObj",  "VOLpxInObj",
+                                "VOLpyInObj",  "VOLpzInObj",  "VOLrhoInObj", "VOLvolumeInObj"};
+const double d3q19_zs_def[24] = {0};
+const char* const d3q19_nt[] = {"XYslice", "XZslice", "YZslice", "EPressure", "Solid", "Wall", "WPressure",
+                                "WPressureL", "WVelocity", "MRT"};
+const int d3q19_nt_v[] = {1, 2, 3, 0x04, 0x08, 0x0C, 0x10, 0x14, 0x18, 0x20};
+const int d3q19_nt_m[] = {3, 3, 3, 0x1C, 0x1C, 0x1C, 0x1C, 0x1C, 0x1C, 0x20};
+const char* const d3q19_q[] = {"P", "U"};
+const int d3q19_qv[] = {0, 1};
+
+const char* const d3q27c_set[] = {"nu", "nubuffer", "GalileanCorrection", "ForceX", "ForceY", "ForceZ", "Omega",
+                                  "Threshold"};
+const double d3q27c_set_def[] = {0.16666666, 0.01, 1, 0, 0, 0, 1, 0.5};
+const int d3q27c_set_der[] = {-1, -1, -1, -1, -1, -1, -1, -1};
+const char* const d3q27c_zs[] = {"Velocity",    "Pressure",   "Turbulence", "DensityInObj",
+                                 "FluxInObj",   "DragInObj",  "LiftInObj",  "LateralInObj",
+                                 "MassInObj",   "XMomentumInObj", "YMomentumInObj", "ZMomentumInObj"};
+const double d3q27c_zs_def[12] = {0};
+const char* const d3q27c_gl[] = {"Density", "Flux", "Drag", "Lift", "Lateral", "Mass", "XMomentum", "YMomentum",
+                                 "ZMomentum", "Objective"};
+const char* const d3q27c_nt[] = {"NSymmetry", "SSymmetry", "Body", "Buffer", "WVelocityTurbulent", "NVelocity",
+                                 "SVelocity", "NPressure", "SPressure", "EPressure", "EVelocity", "Solid", "Wall",
+                                 "WPressure", "WVelocity", "MRT"};
+const int d3q27c_nt_v[] = {1, 2, 4, 0x08, 0x10, 0x18, 0x20, 0x28, 0x30, 0x38, 0x40, 0x48, 0x50, 0x58, 0x60, 0x80};
+const int d3q27c_nt_m[] = {3, 3, 4, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x80};
+const char* const d3q27c_q[] = {"P", "U", "Solid"};
+const int d3q27c_qv[] = {0, 1, 0};
+
+const ModelTable TABLES[3] = {
+    {"d2q9", 9, 2, d2q9::NSET, d2q9::NZS, d2q9::NG, d2q9::NSUM, d2q9::G_Objective, d2q9::IN_OBJ_OFFSET,
+     d2q9::ZONE_SHIFT, d2q9_set, d2q9_set_def, d2q9_set_der, d2q9_zs, d2q9_zs_def, d2q9_gl, d2q9_nt, d2q9_nt_v,
+     d2q9_nt_m, 13, d2q9_q, d2q9_qv, 2},
+    {"d3q19", 19, 3, d3q19::NSET, d3q19::NZS, d3q19::NG, d3q19::NSUM, d3q19::G_Objective, d3q19::IN_OBJ_OFFSET,
+     d3q19::ZONE_SHIFT, d3q19_set, d3q19_set_def, d3q19_set_der, d3q19_zs, d3q19_zs_def, d3q19_gl, d3q19_nt,
+     d3q19_nt_v, d3q19_nt_m, 10, d3q19_q, d3q19_qv, 2},
+    {"d3q27_cumulant", 27, 3, d3q27c::NSET, d3q27c::NZS, d3q27c::NG, d3q27c::NSUM, d3q27c::G_Objective,
+     d3q27c::IN_OBJ_OFFSET, d3q27c::ZONE_SHIFT, d3q27c_set, d3q27c_set_def, d3q27c_set_der, d3q27c_zs, d3q27c_zs_def,
+     d3q27c_gl, d3q27c_nt, d3q27c_nt_v, d3q27c_nt_m, 16, d3q27c_q, d3q27c_qv, 3},
+};
+
+// Derived-setting equations (each model's Dynamics.R AddSetting(..., X='expr'))
+double derive_value(int model, int from, double v) {
+  if (model == MODEL_D2Q9) {
+    if (from == d2q9::S_Viscosity) return 1.0 / (3 * v + 0.5);
+    if (from == d2q9::S_RelaxationRate) return 1 - v;
+  } else if (model == MODEL_D3Q19) {
+    if (from == d3q19::S_nu) return 1.0 / (3 * v + 0.5);
+    if (from == d3q19::S_InletPressure) return 1.0 + v * 3;
+  }
+  return v;
+}
+
+}  // namespace
+
+namespace tclb {
+const ModelTable* model_table(int model) { return (model >= 0 && model < 3) ? &TABLES[model] : nullptr; }
+}  // namespace tclb
+
+// ------------------------------------------------------------------ lattice
+struct Impl;
+
+struct tclb_lattice {
+  int model, precision, storage, device;
+  int nx, ny, nz;
+  size_t N, stride, elem;
+  const ModelTable* T;
+  int nzones;
+  char* pool = nullptr;
+  void* buf[2] = {nullptr, nullptr};
+  int cur = 0;
+  flag_t* flags = nullptr;
+  void* zone_dev = nullptr;
+  double* glob_dev = nullptr;
+  std::vector<double> settings, zone, globals;
+  cudaStream_t stream = nullptr;
+  long long iter = 0;
+  int bx = 128, by = 2;
+  void* qbuf = nullptr;
+  size_t qbuf_bytes = 0;
+  const Impl* impl = nullptr;
+};
+
+struct Impl {
+  void (*iterate)(tclb_lattice*, bool, cudaStream_t);
+  void (*init)(tclb_lattice*, cudaStream_t);
+  void (*quantity)(tclb_lattice*, int, int, const int*, double, void*, cudaStream_t);
+  void (*equilibrium)(tclb_lattice*, const void*, const void*, cudaStream_t);
+  void (*to_double)(const void*, size_t, size_t, size_t, int, double*);   // storage -> double SoA
+  void (*from_double)(const double*, size_t, size_t, size_t, int, void*);  // double SoA -> storage
+  size_t real_size;
+};
+
+namespace {
+
+template <class M, class R>
+Args<R, M::NSET> make_args(const tclb_lattice* L, const void* src, void* dst) {
+  Args<R, M::NSET> a;
+  a.src = src;
+  a.dst = dst;
+  a.stride = L->stride;
+  a.flags = L->flags;
+  a.nx = L->nx;
+  a.ny = L->ny;
+  a.nz = L->nz;
+  a.zone = static_cast<const R*>(L->zone_dev);
+  a.glob = L->glob_dev;
+  for (int i = 0; i < M::NSET; i++) a.s[i] = (R)L->settings[i];
+  return a;
+}
+
+inline dim3 grid_of(const tclb_lattice* L) {
+  return dim3((L->nx + L->bx - 1) / L->bx, (L->ny + L->by - 1) / L->by, L->nz);
+}
+
+template <class M, class R, class St>
+struct Launch {
+  static void iterate(tclb_lattice* L, bool glob, cudaStream_t s) {
+    const void* src = L->buf[L->cur];
+    void* dst = L->buf[1 - L->cur];
+    auto a = make_args<M, R>(L, src, dst);
+    if (glob) k_iterate<M, R, St, true><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a);
+    else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a);
+  }
+  static void init(tclb_lattice* L, cudaStream_t s) {
+    auto a = make_args<M, R>(L, nullptr, L->buf[L->cur]);
+    k_init<M, R, St><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a);
+  }
+  static void quantity(tclb_lattice* L, int q, int vec, const int* r, double scale, void* out, cudaStream_t s) {
+    auto a = make_args<M, R>(L, L->buf[L->cur], nullptr);
+    dim3 blk(32, 4);
+    dim3 grd((r[3] + 31) / 32, (r[4] + 3) / 4, r[5]);
+    k_quantity<M, R, St><<<grd, blk, 0, s>>>(a, q, vec, r[0], r[1], r[2], r[3], r[4], r[5], (R)scale,
+                                               static_cast<R*>(out));
+  }
+  static void equilibrium(tclb_lattice* L, const void* rho, const void* u, cudaStream_t s) {
+    auto a = make_args<M, R>(L, nullptr, L->buf[L->cur]);
+    k_equilibrium<M, R, St><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, static_cast<const R*>(rho),
+                                                                       static_cast<const R*>(u));
+  }
+  static void to_double(const void* raw, size_t N, size_t stride, size_t, int Q, double* out) {
+    const typename St::T* p = static_cast<const typename St::T*>(raw);
+    for (int q = 0; q < Q; q++)
+      for (size_t n = 0; n < N; n++) out[(size_t)q * N + n] = St::to_double(p[(size_t)q * stride + n], M::w(q));
+  }
+  static void from_double(const double* in, size_t N, size_t stride, size_t, int Q, void* raw) {
+    typename St::T* p = static_cast<typename St::T*>(raw);
+    for (int q = 0; q < Q; q++)
+      for (size_t n = 0; n < N; n++) p[(size_t)q * stride + n] = St::from_double(in[(size_t)q * N + n], M::w(q));
+  }
+  static const Impl* get() {
+    static const Impl impl = {iterate, init, quantity, equilibrium, to_double, from_double, sizeof(R)};
+    return &impl;
+  }
+};
+
+template <class M>
+const Impl* impl_for_model(int precision, int storage) {
+  if (precision == TCLB_FP64) return storage == TCLB_STORAGE_SAME ? Launch<M, double, StoreF64>::get() : nullptr;
+  switch (storage) {
+    case TCLB_STORAGE_SAME: return Launch<M, float, StoreF32>::get();
+    case TCLB_STORAGE_FP16: return Launch<M, float, StoreF16<false>>::get();
+    case TCLB_STORAGE_FP16_SHIFT: return Launch<M, float, StoreF16<true>>::get();
+    case TCLB_STORAGE_BF16: return Launch<M, float, StoreBF16<false>>::get();
+    case TCLB_STORAGE_BF16_SHIFT: return Launch<M, float, StoreBF16<true>>::get();
+  }
+  return nullptr;
+}
+
+const Impl* impl_for(int model, int precision, int storage) {
+  switch (model) {
+    case MODEL_D2Q9: return impl_for_model<D2Q9>(precision, storage);
+    case MODEL_D3Q19: return impl_for_model<D3Q19>(precision, storage);
+    case MODEL_D3Q27C: return impl_for_model<D3Q27C>(precision, storage);
+  }
+  return nullptr;
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int upload_zone(tclb_lattice* L) {
+  const size_t n = L->zone.size();
+  if (L->precision == TCLB_FP64) {
+    TCLB_CK(cudaMemcpyAsync(L->zone_dev, L->zone.data(), n * sizeof(double), cudaMemcpyHostToDevice, L->stream));
+  } else {
+    std::vector<float> z(n);
+    for (size_t i = 0; i < n; i++) z[i] = (float)L->zone[i];
+    TCLB_CK(cudaMemcpyAsync(L->zone_dev, z.data(), n * sizeof(float), cudaMemcpyHostToDevice, L->stream));
+    TCLB_CK(cudaStreamSynchronize(L->stream));
+    return TCLB_OK;
+  }
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+int set_setting_rec(tclb_lattice* L, int i, double v, int depth) {
+  if (depth > 8) return fail(TCLB_ERR_STATE, "derived-setting chain too deep");
+  L->settings[i] = v;
+  const int t = L->T->setting_derives[i];
+  if (t >= 0) return set_setting_rec(L, t, derive_value(L->model, i, v), depth + 1);
+  return TCLB_OK;
+}
+
+// Lattice::calcGlobals (src/Lattice.cu.Rt:1299-1315): device Globals -> host
+// accumulators, then clear the device copy.
+int calc_globals(tclb_lattice* L, cudaStream_t s) {
+  std::vector<double> tab(L->T->nglobals);
+  TCLB_CK(cudaMemcpyAsync(tab.data(), L->glob_dev, tab.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < tab.size(); i++) L->globals[i] += tab[i];
+  TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, tab.size() * sizeof(double), s));
+  return TCLB_OK;
+}
+
+#define CHECK_H(h) \
+  if (!(h)) return fail(TCLB_ERR_ARG, "null lattice handle")
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* tclb_last_error(void) { return g_err.c_str(); }
+
+int tclb_model_info(int model, int* Q, int* nsettings, int* nzonesettings, int* nglobals, int* nquantities,
+                    int* zone_shift) {
+  const ModelTable* T = model_table(model);
+  if (!T) return fail(TCLB_ERR_ARG, "unknown model");
+  if (Q) *Q = T->Q;
+  if (nsettings) *nsettings = T->nsettings;
+  if (nzonesettings) *nzonesettings = T->nzonesettings;
+  if (nglobals) *nglobals = T->nglobals;
+  if (nquantities) *nquantities = T->nquantities;
+  if (zone_shift) *zone_shift = T->zone_shift;
+  return TCLB_OK;
+}
+
+int tclb_model_item(int model, int kind, int i, const char** name, int* value, int* mask) {
+  const ModelTable* T = model_table(model);
+  if (!T) return fail(TCLB_ERR_ARG, "unknown model");
+  const char* const* names = nullptr;
+  int n = 0;
+  switch (kind) {
+    case 0: names = T->setting_names; n = T->nsettings; break;
+    case 1: names = T->zone_setting_names; n = T->nzonesettings; break;
+    case 2: names = T->global_names; n = T->nglobals; break;
+    case 3: names = T->node_type_names; n = T->n_node_types; break;
+    case 4: names = T->quantity_names; n = T->nquantities; break;
+    default: return fail(TCLB_ERR_ARG, "unknown item kind");
+  }
+  if (i < 0 || i >= n) return fail(TCLB_ERR_ARG, "item index out of range");
+  if (name) *name = names[i];
+  if (value) *value = kind == 3 ? T->node_type_values[i] : (kind == 4 ? T->quantity_vector[i] : 0);
+  if (mask) *mask = kind == 3 ? T->node_type_masks[i] : 0;
+  return TCLB_OK;
+}
+
+int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, int storage) {
+  if (!out) return fail(TCLB_ERR_ARG, "null output handle");
+  *out = nullptr;
+  const ModelTable* T = model_table(model);
+  if (!T) return fail(TCLB_ERR_ARG, "unknown model");
+  if (nx < 1 || ny < 1 || nz < 1) return fail(TCLB_ERR_ARG, "lattice size must be positive");
+  if (T->dim == 2 && nz != 1) return fail(TCLB_ERR_ARG, "2D model needs nz == 1");
+  if (nz > 65535) return fail(TCLB_ERR_ARG, "nz above 65535");
+  const size_t N = (size_t)nx * ny * nz;
+  if (N >= (size_t)1 << 31) return fail(TCLB_ERR_ARG, "lattice above 2^31 nodes");
+  if (precision != TCLB_FP32 && precision != TCLB_FP64) return fail(TCLB_ERR_ARG, "unknown precision");
+  const Impl* impl = impl_for(model, precision, storage);
+  if (!impl) return fail(TCLB_ERR_ARG, "unsupported precision/storage combination");
+  tclb_lattice* L = new tclb_lattice();
+  L->model = model;
+  L->precision = precision;
+  L->storage = storage;
+  L->nx = nx;
+  L->ny = ny;
+  L->nz = nz;
+  L->N = N;
+  L->T = T;
+  L->impl = impl;
+  L->elem = precision == TCLB_FP64 ? 8 : (storage == TCLB_STORAGE_SAME ? 4 : 2);
+  L->stride = align_up(N, 256 / L->elem);  // 256-byte aligned population planes
+  L->nzones = 1 << (16 - T->zone_shift);
+  cudaGetDevice(&L->device);
+  const size_t bufb = L->stride * T->Q * L->elem;
+  const size_t flagb = align_up(N * sizeof(flag_t), 256);
+  const size_t zoneb = align_up((size_t)L->nzones * T->nzonesettings * impl->real_size, 256);
+  const size_t globb = align_up(T->nglobals * sizeof(double), 256);
+  const size_t total = 2 * bufb + flagb + zoneb + globb;
+  cudaError_t e = cudaMalloc((void**)&L->pool, total);
+  if (e != cudaSuccess) {
+    delete L;
+    cudaGetLastError();
+    return fail(TCLB_ERR_MEMORY, std::string("cudaMalloc of lattice pool failed: ") + cudaGetErrorString(e));
+  }
+  L->buf[0] = L->pool;
+  L->buf[1] = L->pool + bufb;
+  L->flags = reinterpret_cast<flag_t*>(L->pool + 2 * bufb);
+  L->zone_dev = L->pool + 2 * bufb + flagb;
+  L->glob_dev = reinterpret_cast<double*>(L->pool + 2 * bufb + flagb + zoneb);
+  e = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaFree(L->pool);
+    delete L;
+    return fail(TCLB_ERR_CUDA, std::string("stream create failed: ") + cudaGetErrorString(e));
+  }
+  // launch shape: a row of x (multiple of 32), 256 threads per block
+  L->bx = nx >= 128 ? 128 : (nx >= 64 ? 64 : 32);
+  L->by = 256 / L->bx;
+  // settings defaults (src/Solver.cpp.Rt:276-281) and zonal defaults (:393)
+  L->settings.assign(T->nsettings, 0.0);
+  for (int i = 0; i < T->nsettings; i++)
+    if (!std::isnan(T->setting_defaults[i])) L->settings[i] = T->setting_defaults[i];
+  L->zone.assign((size_t)L->nzones * T->nzonesettings, 0.0);
+  for (int z = 0; z < L->nzones; z++)
+    for (int s = 0; s < T->nzonesettings; s++) L->zone[(size_t)z * T->nzonesettings + s] = T->zone_setting_defaults[s];
+  L->globals.assign(T->nglobals, 0.0);
+  int rc = TCLB_OK;
+  if (cudaMemsetAsync(L->pool, 0, total, L->stream) != cudaSuccess) rc = fail(TCLB_ERR_CUDA, "memset of pool failed");
+  if (rc == TCLB_OK) rc = upload_zone(L);
+  if (rc != TCLB_OK) {
+    cudaStreamDestroy(L->stream);
+    cudaFree(L->pool);
+    delete L;
+    return rc;
+  }
+  *out = L;
+  return TCLB_OK;
+}
+
+int tclb_destroy(tclb_h L) {
+  CHECK_H(L);
+  cudaStreamSynchronize(L->stream);
+  if (L->qbuf) cudaFree(L->qbuf);
+  cudaFree(L->pool);
+  cudaStreamDestroy(L->stream);
+  delete L;
+  return TCLB_OK;
+}
+
+int tclb_get_size(tclb_h L, int* nx, int* ny, int* nz) {
+  CHECK_H(L);
+  if (nx) *nx = L->nx;
+  if (ny) *ny = L->ny;
+  if (nz) *nz = L->nz;
+  return TCLB_OK;
+}
+
+int tclb_set_flags(tclb_h L, const uint16_t* flags, int dx, int dy, int dz, int nx, int ny, int nz) {
+  CHECK_H(L);
+  if (!flags) return fail(TCLB_ERR_ARG, "null flags");
+  if (dx < 0 || dy < 0 || dz < 0 || nx < 0 || ny < 0 || nz < 0 || dx + nx > L->nx || dy + ny > L->ny ||
+      dz + nz > L->nz)
+    return fail(TCLB_ERR_ARG, "flag box outside the lattice");
+  if (dx == 0 && dy == 0 && dz == 0 && nx == L->nx && ny == L->ny && nz == L->nz) {
+    TCLB_CK(cudaMemcpyAsync(L->flags, flags, L->N * sizeof(flag_t), cudaMemcpyHostToDevice, L->stream));
+  } else {
+    for (int z = 0; z < nz; z++) {
+      flag_t* d = L->flags + (size_t)dx + (size_t)L->nx * ((size_t)dy + (size_t)L->ny * (dz + z));
+      TCLB_CK(cudaMemcpy2DAsync(d, L->nx * sizeof(flag_t), flags + (size_t)z * nx * ny, nx * sizeof(flag_t),
+                                nx * sizeof(flag_t), ny, cudaMemcpyHostToDevice, L->stream));
+    }
+  }
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+int tclb_get_flags(tclb_h L, uint16_t* flags) {
+  CHECK_H(L);
+  TCLB_CK(cudaMemcpyAsync(flags, L->flags, L->N * sizeof(flag_t), cudaMemcpyDeviceToHost, L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+int tclb_set_setting(tclb_h L, int i, double v) {
+  CHECK_H(L);
+  if (i < 0 || i >= L->T->nsettings) return fail(TCLB_ERR_ARG, "setting index out of range");
+  return set_setting_rec(L, i, v, 0);
+}
+
+int tclb_get_setting(tclb_h L, int i, double* v) {
+  CHECK_H(L);
+  if (i < 0 || i >= L->T->nsettings || !v) return fail(TCLB_ERR_ARG, "setting index out of range");
+  *v = L->settings[i];
+  return TCLB_OK;
+}
+
+int tclb_set_zone_setting(tclb_h L, int s, int zone, double v) {
+  CHECK_H(L);
+  if (s < 0 || s >= L->T->nzonesettings) return fail(TCLB_ERR_ARG, "zone setting index out of range");
+  if (zone < -1 || zone >= L->nzones) return fail(TCLB_ERR_ARG, "zone out of range");
+  const int nzs = L->T->nzonesettings;
+  if (zone < 0)
+    for (int z = 0; z < L->nzones; z++) L->zone[(size_t)z * nzs + s] = v;
+  else
+    L->zone[(size_t)zone * nzs + s] = v;
+  return upload_zone(L);
+}
+
+int tclb_init(tclb_h L) {
+  CHECK_H(L);
+  L->impl->init(L, L->stream);
+  TCLB_CK(cudaGetLastError());
+  L->iter = 0;
+  std::fill(L->globals.begin(), L->globals.end(), 0.0);
+  TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, L->T->nglobals * sizeof(double), L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+int tclb_init_equilibrium(tclb_h L, const void* rho, const void* u, void* stream) {
+  CHECK_H(L);
+  if (!rho || !u) return fail(TCLB_ERR_ARG, "null field");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const size_t rs = L->impl->real_size;
+  const size_t bytes = align_up(L->N * rs, 256) + 3 * L->N * rs;
+  if (bytes > L->qbuf_bytes) {
+    if (L->qbuf) TCLB_CK(cudaFree(L->qbuf));
+    L->qbuf = nullptr;
+    L->qbuf_bytes = 0;
+    TCLB_CK(cudaMalloc(&L->qbuf, bytes));
+    L->qbuf_bytes = bytes;
+  }
+  char* d_rho = static_cast<char*>(L->qbuf);
+  char* d_u = d_rho + align_up(L->N * rs, 256);
+  TCLB_CK(cudaMemcpyAsync(d_rho, rho, L->N * rs, cudaMemcpyHostToDevice, s));
+  TCLB_CK(cudaMemcpyAsync(d_u, u, 3 * L->N * rs, cudaMemcpyHostToDevice, s));
+  L->impl->equilibrium(L, d_rho, d_u, s);
+  TCLB_CK(cudaGetLastError());
+  L->iter = 0;
+  std::fill(L->globals.begin(), L->globals.end(), 0.0);
+  TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, L->T->nglobals * sizeof(double), s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
+int tclb_iterate(tclb_h L, int niter, int iter_type, void* stream) {
+  CHECK_H(L);
+  if (niter < 0) return fail(TCLB_ERR_ARG, "negative iteration count");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  int last_glob = iter_type & TCLB_ITER_LASTGLOB;
+  const bool integ = (iter_type & TCLB_ITER_INTEG) == TCLB_ITER_INTEG;
+  if (integ) last_glob = 0;
+  bool globs = (iter_type & TCLB_ITER_GLOBS) != 0;
+  for (int i = 0; i < niter; i++) {
+    if (last_glob && i == niter - 1) {
+      TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, L->T->nglobals * sizeof(double), s));
+      globs = true;
+    }
+    L->impl->iterate(L, globs, s);
+    L->cur = 1 - L->cur;
+    L->iter++;
+  }
+  TCLB_CK(cudaGetLastError());
+  if (last_glob && niter > 0) {
+    std::fill(L->globals.begin(), L->globals.end(), 0.0);
+    return calc_globals(L, s);
+  } else if (integ && niter > 0) {
+    return calc_globals(L, s);
+  }
+  return TCLB_OK;
+}
+
+int tclb_get_globals(tclb_h L, double* out) {
+  CHECK_H(L);
+  if (!out) return fail(TCLB_ERR_ARG, "null output");
+  std::copy(L->globals.begin(), L->globals.end(), out);
+  return TCLB_OK;
+}
+
+int tclb_clear_globals(tclb_h L) {
+  CHECK_H(L);
+  std::fill(L->globals.begin(), L->globals.end(), 0.0);
+  return TCLB_OK;
+}
+
+int tclb_get_quantity(tclb_h L, int q, const int region[6], void* out, double scale, void* stream) {
+  CHECK_H(L);
+  if (q < 0 || q >= L->T->nquantities) return fail(TCLB_ERR_ARG, "quantity index out of range");
+  if (!out) return fail(TCLB_ERR_ARG, "null output");
+  int r[6] = {0, 0, 0, L->nx, L->ny, L->nz};
+  if (region) std::memcpy(r, region, sizeof(r));
+  if (r[0] < 0 || r[1] < 0 || r[2] < 0 || r[3] < 1 || r[4] < 1 || r[5] < 1 || r[0] + r[3] > L->nx ||
+      r[1] + r[4] > L->ny || r[2] + r[5] > L->nz)
+    return fail(TCLB_ERR_ARG, "quantity region outside the lattice");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const int vec = L->T->quantity_vector[q];
+  const size_t bytes = (size_t)r[3] * r[4] * r[5] * (vec ? 3 : 1) * L->impl->real_size;
+  if (bytes > L->qbuf_bytes) {
+    if (L->qbuf) TCLB_CK(cudaFree(L->qbuf));
+    L->qbuf = nullptr;
+    L->qbuf_bytes = 0;
+    TCLB_CK(cudaMalloc(&L->qbuf, bytes));
+    L->qbuf_bytes = bytes;
+  }
+  L->impl->quantity(L, q, vec, r, scale, L->qbuf, s);
+  TCLB_CK(cudaGetLastError());
+  TCLB_CK(cudaMemcpyAsync(out, L->qbuf, bytes, cudaMemcpyDeviceToHost, s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
+int tclb_get_densities(tclb_h L, double* out) {
+  CHECK_H(L);
+  if (!out) return fail(TCLB_ERR_ARG, "null output");
+  std::vector<char> raw(L->stride * L->T->Q * L->elem);
+  TCLB_CK(cudaMemcpyAsync(raw.data(), L->buf[L->cur], raw.size(), cudaMemcpyDeviceToHost, L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  L->impl->to_double(raw.data(), L->N, L->stride, L->elem, L->T->Q, out);
+  return TCLB_OK;
+}
+
+int tclb_set_densities(tclb_h L, const double* in) {
+  CHECK_H(L);
+  if (!in) return fail(TCLB_ERR_ARG, "null input");
+  std::vector<char> raw(L->stride * L->T->Q * L->elem, 0);
+  L->impl->from_double(in, L->N, L->stride, L->elem, L->T->Q, raw.data());
+  TCLB_CK(cudaMemcpyAsync(L->buf[L->cur], raw.data(), raw.size(), cudaMemcpyHostToDevice, L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+size_t tclb_snapshot_bytes(tclb_h L) { return L ? L->N * L->T->Q * L->elem : 0; }
+
+int tclb_save(tclb_h L, void* host, size_t bytes, void* stream) {
+  CHECK_H(L);
+  if (!host || bytes != tclb_snapshot_bytes(L)) return fail(TCLB_ERR_ARG, "snapshot buffer size mismatch");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const size_t plane = L->N * L->elem;
+  if (L->stride == L->N) {
+    TCLB_CK(cudaMemcpyAsync(host, L->buf[L->cur], bytes, cudaMemcpyDeviceToHost, s));
+  } else {
+    for (int q = 0; q < L->T->Q; q++)
+      TCLB_CK(cudaMemcpyAsync(static_cast<char*>(host) + q * plane,
+                              static_cast<char*>(L->buf[L->cur]) + q * L->stride * L->elem, plane,
+                              cudaMemcpyDeviceToHost, s));
+  }
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
+int tclb_load(tclb_h L, const void* host, size_t bytes, void* stream) {
+  CHECK_H(L);
+  if (!host || bytes != tclb_snapshot_bytes(L)) return fail(TCLB_ERR_ARG, "snapshot buffer size mismatch");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const size_t plane = L->N * L->elem;
+  if (L->stride == L->N) {
+    TCLB_CK(cudaMemcpyAsync(L->buf[L->cur], host, bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    for (int q = 0; q < L->T->Q; q++)
+      TCLB_CK(cudaMemcpyAsync(static_cast<char*>(L->buf[L->cur]) + q * L->stride * L->elem,
+                              static_cast<const char*>(host) + q * plane, plane, cudaMemcpyHostToDevice, s));
+  }
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
+int tclb_get_iteration(tclb_h L, long long* iter) {
+  CHECK_H(L);
+  if (iter) *iter = L->iter;
+  return TCLB_OK;
+}
+
+double tclb_bytes_per_update(tclb_h L) { return L ? 2.0 * L->T->Q * L->elem + sizeof(flag_t) : 0.0; }
+
+int tclb_sync(tclb_h L) {
+  CHECK_H(L);
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+}  // extern "C"

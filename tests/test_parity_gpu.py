@@ -1,0 +1,237 @@
+"""Parity of the CUDA library (through its C ABI) against the CPU oracle.
+
+Tolerances: FP64 path relative L2 <= 1e-12 on densities (the north-star bar
+against TCLB's double build); FP32 path <= 1e-5 relative L2 on velocity and
+densities (the bar against TCLB's float build). Globals: FP64 1e-10 relative,
+FP32 1e-4 relative (FP64 sums of FP32 per-node values).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tclb_b200 import cases
+from tclb_b200 import models as M
+from tclb_b200.lattice import Lattice, TCLBError
+
+from helpers import apply_params, perturbed_equilibrium, random_flags, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_F = {"fp64": 1e-12, "fp32": 1e-5}
+TOL_G = {"fp64": 1e-10, "fp32": 1e-4}
+
+BOUNDARY_TYPES = {
+    "d2q9": ["EPressure", "WPressure", "NVelocity", "SVelocity", "WVelocity", "EVelocity", "NSymmetry", "SSymmetry",
+             "Solid", "Wall"],
+    "d3q19": ["EPressure", "Solid", "Wall", "WPressure", "WPressureL", "WVelocity"],
+    "d3q27_cumulant": ["Buffer", "WVelocityTurbulent", "NVelocity", "SVelocity", "NPressure", "SPressure",
+                       "EPressure", "EVelocity", "Solid", "Wall", "WPressure", "WVelocity"],
+}
+EXTRA_GROUPS = {"d2q9": ["OBJECTIVE"], "d3q19": ["ADDITIONALS"], "d3q27_cumulant": ["ADDITIONALS", "BODY"]}
+
+PARAMS = {
+    "d2q9": [("setting", "Viscosity", 0.05), ("setting", "S3", 0.3), ("setting", "S4", -0.2),
+             ("setting", "GravitationX", 1e-5), ("setting", "GravitationY", -2e-6),
+             ("zone", "VelocityX", 0.02, 0), ("zone", "VelocityX", 0.03, 1), ("zone", "VelocityY", 0.005, 2),
+             ("zone", "Pressure", 0.01, 1), ("zone", "Pressure", -0.005, 2),
+             ("zone", "OutletFluxInObj", 0.5, 1), ("zone", "PressureLossInObj", 2.0, 2)],
+    "d3q19": [("setting", "nu", 0.05), ("setting", "InletVelocity", 0.02), ("setting", "InletPressure", 0.01),
+              ("setting", "ForceX", 1e-5), ("setting", "ForceZ", -3e-6), ("zone", "VOLvxInObj", 1.5, 1)],
+    "d3q27_cumulant": [("setting", "nu", 0.02), ("setting", "nubuffer", 0.05), ("setting", "ForceX", 1e-5),
+                       ("setting", "ForceY", 2e-6), ("setting", "Omega", 0.8),
+                       ("zone", "Velocity", 0.02, 0), ("zone", "Velocity", 0.03, 1), ("zone", "Pressure", 0.01, 2),
+                       ("zone", "DragInObj", 0.7, 1)],
+}
+
+
+def make_pair(model, shape, precision, storage="same"):
+    nz, ny, nx = shape
+    g = Lattice(model, nx, ny, nz, precision=precision, storage=storage)
+    o = oracle.OracleLattice(model, nx, ny, nz, precision="fp64" if precision == "fp64" else "fp32")
+    return g, o
+
+
+def run_both(g, o, niter, iter_type):
+    g.Iterate(niter, iter_type)
+    o.iterate(niter, iter_type)
+
+
+def compare_globals(g, o, precision, atol=1e-12):
+    gg, og = g.globals, o.globals()
+    scale = np.maximum(np.abs(og), atol)
+    err = np.abs(gg - og) / scale
+    return float(err.max()), gg, og
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_all_node_types(model, precision):
+    """Every boundary type, zone and extra group on random nodes; a few
+    iterations from a perturbed equilibrium; Globals on the last one."""
+    m = M.get(model)
+    shape = (1, 24, 64) if m.dim == 2 else (12, 10, 32)
+    fl = random_flags(model, shape, BOUNDARY_TYPES[model], zones=3, seed=1, p_type=0.35,
+                      extra_groups=EXTRA_GROUPS[model])
+    f0 = perturbed_equilibrium(model, shape, seed=2)
+    g, o = make_pair(model, shape, precision)
+    for lat in (g, o):
+        lat.set_flags(fl)
+        apply_params(lat, PARAMS[model])
+        lat.set_densities(f0)
+    run_both(g, o, 6, M.ITER_NORM | M.ITER_LASTGLOB)
+    e = rel_l2(g.densities(), o.densities())
+    assert e < TOL_F[precision], f"densities rel L2 {e:.3e}"
+    ge, gg, og = compare_globals(g, o, precision)
+    assert ge < TOL_G[precision], f"globals rel err {ge:.3e}\n{gg}\n{og}"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_init_and_quantities(model, precision):
+    m = M.get(model)
+    shape = (1, 16, 64) if m.dim == 2 else (8, 8, 32)
+    fl = random_flags(model, shape, BOUNDARY_TYPES[model], zones=3, seed=5, p_type=0.3,
+                      extra_groups=EXTRA_GROUPS[model])
+    g, o = make_pair(model, shape, precision)
+    for lat in (g, o):
+        lat.set_flags(fl)
+        apply_params(lat, PARAMS[model])
+        lat.Init() if hasattr(lat, "Init") else lat.init()
+    tol = TOL_F[precision]
+    assert rel_l2(g.densities(), o.densities()) < tol
+    run_both(g, o, 3, M.ITER_NORM)
+    for qi, (qn, vec) in enumerate(m.quantities):
+        a = g.GetQuantity(qn)
+        b = o.quantity(qn)
+        if np.linalg.norm(b) == 0:
+            assert np.abs(a).max() < tol
+        else:
+            assert rel_l2(a, b) < 10 * tol, f"quantity {qn}"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_channel_disc_d2q9(precision):
+    """Configuration 1 at reduced size: 256x64 channel, disc r=8, 500 iterations,
+    Globals every 100 (ITER_LASTGLOB)."""
+    nx, ny = 256, 64
+    fl = cases.channel_disc_d2q9(nx, ny, r=8, cx=64, cy=32)
+    g, o = make_pair("d2q9", (1, ny, nx), precision)
+    for lat in (g, o):
+        lat.set_flags(fl)
+        apply_params(lat, cases.channel_disc_settings(ux=0.01, nu=0.02, bgk=True))
+        lat.Init() if hasattr(lat, "Init") else lat.init()
+    for _ in range(5):
+        run_both(g, o, 100, M.ITER_NORM | M.ITER_LASTGLOB)
+        ge, gg, og = compare_globals(g, o, precision)
+        assert ge < TOL_G[precision], f"globals {gg} vs {og}"
+    u_g, u_o = g.GetQuantity("U"), o.quantity("U")
+    assert rel_l2(u_g, u_o) < TOL_F[precision]
+    assert rel_l2(g.densities(), o.densities()) < TOL_F[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_tgv_d3q27(precision):
+    """Configuration 2 at 32^3: Taylor-Green vortex, 100 iterations."""
+    n = 32
+    rho, u = cases.tgv_fields(n, u0=0.05, dtype=np.float64)
+    # equilibrium populations from (rho, rho*u) on the host
+    w = np.array(M.get("d3q27_cumulant").weights)
+    e = np.array(M.get("d3q27_cumulant").velocities, np.float64)
+    J = rho[..., None] * u
+    eu = np.einsum("qd,zyxd->qzyx", e, J)
+    j2 = (J ** 2).sum(-1)
+    f = w[:, None, None, None] * (rho + 3 * eu + 4.5 * eu ** 2 / rho - 1.5 * j2 / rho)
+    g, o = make_pair("d3q27_cumulant", (n, n, n), precision)
+    for lat in (g, o):
+        lat.set_flags(cases.tgv_flags("d3q27_cumulant", n))
+        lat.set_setting("nu", 1e-3)
+        lat.set_densities(f)
+    for _ in range(2):
+        run_both(g, o, 50, M.ITER_NORM | M.ITER_LASTGLOB)
+        ge, gg, og = compare_globals(g, o, precision)
+        assert ge < TOL_G[precision], f"{gg} vs {og}"
+    assert rel_l2(g.GetQuantity("U"), o.quantity("U")) < TOL_F[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_porous_d3q19(precision):
+    """Configuration 3 at 64x32x32: porous channel with body force, 200 iterations."""
+    nx, ny, nz = 64, 32, 32
+    fl = cases.porous_channel_d3q19(nx, ny, nz, p=0.08, band=4, seed=3)
+    g, o = make_pair("d3q19", (nz, ny, nx), precision)
+    for lat in (g, o):
+        lat.set_flags(fl)
+        apply_params(lat, [("setting", "nu", 0.01), ("setting", "ForceX", 1e-5)])
+        lat.Init() if hasattr(lat, "Init") else lat.init()
+    run_both(g, o, 200, M.ITER_NORM | M.ITER_LASTGLOB)
+    assert rel_l2(g.GetQuantity("U"), o.quantity("U")) < TOL_F[precision]
+    ge, gg, og = compare_globals(g, o, precision)
+    assert ge < TOL_G[precision], f"{gg} vs {og}"
+
+
+@pytest.mark.parametrize("storage", ["fp16s", "bf16s", "fp16", "bf16"])
+def test_reduced_storage_d3q19(storage):
+    """Reduced-precision storage against the FP64 oracle: velocity error bound."""
+    nx, ny, nz = 64, 32, 32
+    fl = cases.porous_channel_d3q19(nx, ny, nz, p=0.08, band=4, seed=3)
+    g = Lattice("d3q19", nx, ny, nz, precision="fp32", storage=storage)
+    o = oracle.OracleLattice("d3q19", nx, ny, nz, precision="fp64")
+    for lat in (g, o):
+        lat.set_flags(fl)
+        apply_params(lat, [("setting", "nu", 0.01), ("setting", "ForceX", 1e-5)])
+        lat.Init() if hasattr(lat, "Init") else lat.init()
+    run_both(g, o, 200, M.ITER_NORM)
+    err = rel_l2(g.GetQuantity("U"), o.quantity("U"))
+    bound = {"fp16s": 1e-2, "bf16s": 1e-1, "fp16": 5e-1, "bf16": 2.0}[storage]
+    assert err < bound, f"{storage}: velocity rel L2 {err:.3e}"
+
+
+def test_globals_cadence():
+    """ITER_LASTGLOB replaces the host Globals with the last iteration's;
+    ITER_INTEG integrates every iteration and accumulates across calls
+    (src/Lattice.cu.Rt:900-989)."""
+    shape = (8, 8, 32)
+    g, o = make_pair("d3q27_cumulant", shape, "fp64")
+    for lat in (g, o):
+        lat.set_flags(cases.tgv_flags("d3q27_cumulant", 32, nz=8)[:, :8, :])
+        lat.set_densities(perturbed_equilibrium("d3q27_cumulant", shape, seed=9))
+    for it in (M.ITER_NORM | M.ITER_LASTGLOB, M.ITER_INTEG, M.ITER_INTEG, M.ITER_NORM, M.ITER_NORM | M.ITER_LASTGLOB):
+        run_both(g, o, 3, it)
+        ge, gg, og = compare_globals(g, o, "fp64")
+        assert ge < 1e-10, (it, gg, og)
+
+
+def test_save_load_roundtrip():
+    g = Lattice("d3q19", 32, 8, 8, precision="fp32", storage="fp16s")
+    g.set_flags(np.full((8, 8, 32), M.get("d3q19").flag("MRT"), np.uint16))
+    g.Init()
+    g.Iterate(3)
+    snap = g.save()
+    d0 = g.densities()
+    g.Iterate(2)
+    g.load(snap)
+    assert np.array_equal(g.densities(), d0)
+    assert snap.nbytes == 19 * 32 * 8 * 8 * 2
+
+
+def test_flag_subbox():
+    m = M.get("d2q9")
+    g = Lattice("d2q9", 64, 16)
+    full = np.full((1, 16, 64), m.flag("MRT"), np.uint16)
+    g.FlagOverwrite(full)
+    box = np.full((1, 4, 8), m.flag("Wall"), np.uint16)
+    g.FlagOverwrite(box, offset=(10, 3, 0))
+    full[:, 3:7, 10:18] = m.flag("Wall")
+    assert np.array_equal(g.get_flags(), full)
+
+
+def test_errors_are_status_codes():
+    with pytest.raises(TCLBError):
+        Lattice("d2q9", 64, 16, 2)  # 2D model with nz > 1
+    with pytest.raises(TCLBError):
+        Lattice("d3q19", 16, 16, 16, precision="fp64", storage="fp16s")
+    g = Lattice("d2q9", 64, 16)
+    with pytest.raises(TCLBError):
+        g.GetQuantity("U", region=[60, 0, 0, 8, 16, 1])
+    with pytest.raises(TCLBError):
+        g.FlagOverwrite(np.zeros((1, 4, 8), np.uint16), offset=(60, 0, 0))
