@@ -251,8 +251,12 @@ def run_ours(args):
 
     lat = Lattice(args.model, n, n, n, precision=args.precision, storage=args.storage)
     tgv_setup(lat, n)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the library launches on it, the CUDA
+    # events below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    assert sp != 0
     N = lat.N
     bpu = lat.bytes_per_update
 

@@ -44,6 +44,7 @@ def lib():
         L.orc_init.argtypes = [vp]
         L.orc_iterate.argtypes = [vp, i, i]
         L.orc_get_globals.argtypes = [vp, dp]
+        L.orc_get_globals_scale.argtypes = [vp, dp]
         L.orc_get_quantity.argtypes = [vp, i, dp]
         L.orc_get_densities.argtypes = [vp, dp]
         L.orc_set_densities.argtypes = [vp, dp]
@@ -112,6 +113,12 @@ class OracleLattice:
     def globals(self) -> np.ndarray:
         out = np.zeros(len(self.model.globals))
         lib().orc_get_globals(self._h, _dp(out))
+        return out
+
+    def globals_scale(self) -> np.ndarray:
+        """Sum of |contribution| per Global: the scale for comparing sums."""
+        out = np.zeros(len(self.model.globals))
+        lib().orc_get_globals_scale(self._h, _dp(out))
         return out
 
     def quantity(self, name) -> np.ndarray:

@@ -500,6 +500,9 @@ struct Lattice {
   std::vector<double> settings;
   std::vector<double> zone;  // zones * nzs
   int nzones;
+  // Globals are kept as 2*nglob values: the sums, then the sums of absolute
+  // contributions (the scale against which summation and rounding differences
+  // are judged by the tests).
   std::vector<double> dev_globals;  // per-iteration integrated globals (device side in TCLB)
   std::vector<double> globals;      // host accumulators (Lattice::globals)
   long iter = 0;
@@ -519,8 +522,8 @@ struct Lattice {
     zone.assign((size_t)nzones * I.nzs, 0.0);
     for (int z = 0; z < nzones; z++)
       for (int s = 0; s < I.nzs; s++) zone[(size_t)z * I.nzs + s] = I.zs_default[s];
-    dev_globals.assign(I.nglob, 0.0);
-    globals.assign(I.nglob, 0.0);
+    dev_globals.assign(2 * I.nglob, 0.0);
+    globals.assign(2 * I.nglob, 0.0);
   }
 
   void set_setting(int i, double v) {  // Lattice::SetSetting (src/Lattice.cu.Rt:1350-1358)
@@ -534,10 +537,19 @@ struct Lattice {
 
   // AddTo<G>(x): value plus the Objective quirk (src/cuda.cu.Rt:114-119).
   inline void add(std::vector<double>& g, int gi, R x, flag_t fl) const {
+    const int ng = ops.info.nglob;
     g[gi] += (double)x;
-    if (gi < ops.info.nsum) g[ops.info.obj_idx] += (double)Z(gi + ops.info.in_obj_offset, fl);
+    g[ng + gi] += std::fabs((double)x);
+    if (gi < ops.info.nsum) {
+      const double w = (double)Z(gi + ops.info.in_obj_offset, fl);
+      g[ops.info.obj_idx] += w;
+      g[ng + ops.info.obj_idx] += std::fabs(w);
+    }
   }
-  inline void maxg(std::vector<double>& g, int gi, R x) const { g[gi] = std::max(g[gi], (double)x); }
+  inline void maxg(std::vector<double>& g, int gi, R x) const {
+    g[gi] = std::max(g[gi], (double)x);
+    g[ops.info.nglob + gi] = std::max(g[ops.info.nglob + gi], std::fabs((double)x));
+  }
 
   // ---------------- d2q9 (models/flow/d2q9/Dynamics.c.Rt) ----------------
   void feq_fill(R* f, R rho, const R* J) const {
@@ -1054,7 +1066,7 @@ struct Lattice {
 #ifdef _OPENMP
     nthreads = omp_get_max_threads();
 #endif
-    std::vector<std::vector<double>> part(nthreads, std::vector<double>(ng, 0.0));
+    std::vector<std::vector<double>> part(nthreads, std::vector<double>(2 * ng, 0.0));
 #pragma omp parallel for collapse(2) schedule(static)
     for (int z = 0; z < nz; z++)
       for (int y = 0; y < ny; y++) {
@@ -1073,8 +1085,8 @@ struct Lattice {
       }
     if (glob) {
       for (int t = 0; t < nthreads; t++)
-        for (int g = 0; g < ng; g++) {
-          if (g < ops.info.nsum) dev_globals[g] += part[t][g];
+        for (int g = 0; g < 2 * ng; g++) {
+          if (g % ng < ops.info.nsum) dev_globals[g] += part[t][g];
           else dev_globals[g] = std::max(dev_globals[g], part[t][g]);
         }
     }
@@ -1259,7 +1271,15 @@ int orc_iterate(void* p, int niter, int iter_type) {
 
 int orc_get_globals(void* p, double* out) {
   Handle* h = (Handle*)p;
-  auto f = [&](auto* L) { std::copy(L->globals.begin(), L->globals.end(), out); };
+  auto f = [&](auto* L) { std::copy(L->globals.begin(), L->globals.begin() + L->ops.info.nglob, out); };
+  if (h->precision) f(h->ld); else f(h->lf);
+  return 0;
+}
+
+// Sum of absolute contributions of each Global (its error scale), same cadence.
+int orc_get_globals_scale(void* p, double* out) {
+  Handle* h = (Handle*)p;
+  auto f = [&](auto* L) { std::copy(L->globals.begin() + L->ops.info.nglob, L->globals.end(), out); };
   if (h->precision) f(h->ld); else f(h->lf);
   return 0;
 }
