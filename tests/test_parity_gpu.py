@@ -10,8 +10,9 @@ Tolerances (written here, used below):
   eps32*rho/|u| times the random walk over the iterations sets a 1e-4 bar.
 * Globals: |difference| <= tol * sum_i |x_i| (sum of absolute per-node
   contributions, from the oracle) -- the scale that bounds summation and
-  rounding differences; tol = 1e-10 for FP64, 1e-3 for FP32 (per-node FP32
-  values such as d2q9's (rho-1)/3 lose about three digits to cancellation).
+  rounding differences; tol = 1e-10 for FP64, 3e-3 for FP32 (per-node FP32
+  values such as d2q9's (rho-1)/3 with rho-1 ~ 1e-3 lose about three digits to
+  cancellation, so FP32 state differences of ~1e-6 show up at ~1e-3 there).
 """
 import numpy as np
 import pytest
@@ -27,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 TOL_F = {"fp64": 1e-12, "fp32": 1e-5}
 TOL_U = {"fp64": 1e-11, "fp32": 1e-5}
-TOL_G = {"fp64": 1e-10, "fp32": 1e-3}
+TOL_G = {"fp64": 1e-10, "fp32": 3e-3}
 
 BOUNDARY_TYPES = {
     "d2q9": ["EPressure", "WPressure", "NVelocity", "SVelocity", "WVelocity", "EVelocity", "NSymmetry", "SSymmetry",
