@@ -114,6 +114,21 @@ int tclb_clear_globals(tclb_h h);
    TCLB_FP32, double for TCLB_FP64); vector quantities are 3 values per node. */
 int tclb_get_quantity(tclb_h h, int q, const int region[6], void* out, double scale, void* stream);
 
+/* Same result as tclb_get_quantity, for callers that must not allocate device
+   memory: an application whose GPU memory is all owned by its own pool or
+   admission budget, or a latency-critical loop where cudaMalloc/cudaFree would
+   synchronise the device. No counterpart in the reference (TCLB's GetQuantity
+   allocates a buffer on every call, src/Lattice.cu.Rt:1210-1220).
+   It stages the quantity in a fixed 8 MiB device array compiled into the
+   library (held by every GPU that loads the library until the process exits)
+   and calls no cudaMalloc/cudaFree. Regions whose quantity needs more than
+   8 MiB (nodes x components x sizeof(real_t)) are rejected with
+   TCLB_ERR_ARG. The first call on a device looks up the array's device
+   address (cudaGetSymbolAddress) and caches it; make that first call before
+   any stream capture. All calls share the array: calls that overlap on the
+   GPU race. */
+int tclb_get_quantity_noalloc(tclb_h h, int q, const int region[6], void* out, double scale, void* stream);
+
 /* Get_/Set_<field> for all densities at once: SoA [q][z][y][x] as double. */
 int tclb_get_densities(tclb_h h, double* out);
 int tclb_set_densities(tclb_h h, const double* in);

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -634,3 +635,82 @@ int tclb_sync(tclb_h L) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Quantity read-out that allocates no device memory.
+//
+// tclb_get_quantity stages the quantity in a device buffer that it grows with
+// cudaMalloc. Some callers cannot allow that: a host application that has
+// handed the whole GPU to its own memory pool or admission budget (a
+// cudaMalloc there can fail, or break the budget the pool enforces), and code
+// on a latency-critical path, where cudaMalloc/cudaFree may synchronise the
+// device and stall unrelated streams. For them this variant stages the
+// quantity in a fixed device array that is part of the library image.
+//
+// The array is TCLB_NOALLOC_SCRATCH_BYTES (8 MiB) of device memory held by
+// every GPU that loads the library, until the process exits. Regions whose
+// quantity needs more are rejected. All calls share the array and it keeps
+// the last call's contents; the quantity kernel overwrites every byte a call
+// reads back, so nothing needs clearing. Calls that overlap on the GPU (other
+// host threads, or other streams without ordering between them) race on the
+// array.
+// ---------------------------------------------------------------------------
+#define TCLB_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define TCLB_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[TCLB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[TCLB_NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_noalloc_scratch on `dev`, which must be current. In host
+// code the array's name is only a host-side stand-in, so the address is looked
+// up once per device with cudaGetSymbolAddress and cached.
+int noalloc_scratch(int dev, void** out) {
+  if (dev < 0 || dev >= TCLB_NOALLOC_MAX_DEVICES) return fail(TCLB_ERR_ARG, "device ordinal above the no-allocation table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_address[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(TCLB_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(e));
+    g_noalloc_address[dev] = p;
+  }
+  *out = g_noalloc_address[dev];
+  return TCLB_OK;
+}
+}  // namespace
+
+extern "C" int tclb_get_quantity_noalloc(tclb_h L, int q, const int region[6], void* out, double scale,
+                                         void* stream) {
+  CHECK_H(L);
+  if (q < 0 || q >= L->T->nquantities) return fail(TCLB_ERR_ARG, "quantity index out of range");
+  if (!out) return fail(TCLB_ERR_ARG, "null output");
+  int r[6] = {0, 0, 0, L->nx, L->ny, L->nz};
+  if (region) std::memcpy(r, region, sizeof(r));
+  if (r[0] < 0 || r[1] < 0 || r[2] < 0 || r[3] < 1 || r[4] < 1 || r[5] < 1 || r[0] + r[3] > L->nx ||
+      r[1] + r[4] > L->ny || r[2] + r[5] > L->nz)
+    return fail(TCLB_ERR_ARG, "quantity region outside the lattice");
+  const int vec = L->T->quantity_vector[q];
+  const size_t bytes = (size_t)r[3] * r[4] * r[5] * (vec ? 3 : 1) * L->impl->real_size;
+  if (bytes > TCLB_NOALLOC_SCRATCH_BYTES)
+    return fail(TCLB_ERR_ARG, "region needs " + std::to_string(bytes) +
+                                  " bytes of scratch, above the no-allocation limit of " +
+                                  std::to_string(TCLB_NOALLOC_SCRATCH_BYTES) + " bytes; use tclb_get_quantity");
+  int prev = -1;
+  TCLB_CK(cudaGetDevice(&prev));
+  if (prev != L->device) TCLB_CK(cudaSetDevice(L->device));
+  void* scratch = nullptr;
+  int rc = noalloc_scratch(L->device, &scratch);
+  if (rc == TCLB_OK) {
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+    L->impl->quantity(L, q, vec, r, scale, scratch, s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, scratch, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(TCLB_ERR_CUDA, std::string("no-allocation quantity: ") + cudaGetErrorString(e));
+  }
+  if (prev != L->device) cudaSetDevice(prev);
+  return rc;
+}
