@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--config", type=int, default=2,
+                   help="2 = the headline Taylor-Green line; 1, 3, 4, 5 = the other configurations (one JSON line)")
     return p.parse_args()
 
 
@@ -349,10 +351,25 @@ def run_ours(args):
     return 0
 
 
+def run_config(args):
+    import torch
+
+    from tclb_b200 import benchmarks as BM
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    fn = {1: BM.config1, 3: BM.config3, 4: BM.config4, 5: BM.config5}[args.config]
+    res = fn()
+    print(json.dumps({"metric": METRIC, "unit": UNIT, "config_id": args.config, "data": "synthetic", **res}),
+          flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config != 2:
+        return run_config(args)
     return run_ours(args)
 
 

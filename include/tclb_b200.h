@@ -147,6 +147,55 @@ double tclb_bytes_per_update(tclb_h h);
 /* Synchronise the lattice's stream. */
 int tclb_sync(tclb_h h);
 
+/* Launch shape of the iteration kernel (bx multiple of 32, bx*by <= 256) and
+   whether runs of plain iterations replay a captured CUDA graph (default on). */
+int tclb_set_launch(tclb_h h, int bx, int by, int use_graphs);
+
+/* ---------------------------------------------------------------------------
+   Batches: many independent cases of one model advanced together by one
+   persistent, CUDA-graph-captured launch per replay. No counterpart in the
+   reference, which runs one lattice per process (src/main.cpp:173-425).
+   ------------------------------------------------------------------------- */
+typedef struct tclb_batch* tclb_batch_h;
+
+const char* tclb_batch_last_error(void);
+
+/* Device bytes one case occupies (two snapshots, node types, zonal table,
+   Globals): the footprint admission is judged on. */
+size_t tclb_batch_case_bytes(int model, int precision, int storage, int nx, int ny, int nz);
+
+/* A batch admits cases while the sum of their footprints stays within
+   budget_bytes and at most max_cases are resident. */
+int tclb_batch_create(tclb_batch_h* out, int model, int precision, int storage, size_t budget_bytes, int max_cases);
+int tclb_batch_destroy(tclb_batch_h b);
+
+/* Admit a case: node types (x fastest), the full Settings vector (derived
+   chains already applied), `zone_rows` rows of ZoneSettings (zone 0..), and
+   the number of iterations to run. The case starts at its BaseInit
+   equilibrium. TCLB_ERR_MEMORY when the budget or the slots are exhausted. */
+int tclb_batch_add_case(tclb_batch_h b, int nx, int ny, int nz, const uint16_t* flags, const double* settings,
+                        const double* zone_settings, int zone_rows, int niter, int* case_id);
+/* Retire a case and return its memory to the batch's pool (stream-ordered). */
+int tclb_batch_remove_case(tclb_batch_h b, int case_id);
+
+/* Launch shape: tile bx x by nodes per block (bx multiple of 32, bx*by <= 256),
+   iterations per replay, persistent grid size (0 = SMs x resident blocks). */
+int tclb_batch_set_launch(tclb_batch_h b, int bx, int by, int iters_per_launch, int grid_blocks);
+int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launch);
+
+/* Enqueue one replay (asynchronous); every active case advances by
+   min(iters_per_launch, remaining) iterations; Globals are those of each case's
+   last iteration in the replay. */
+int tclb_batch_step(tclb_batch_h b);
+int tclb_batch_sync(tclb_batch_h b);
+/* After tclb_batch_sync: iterations done / left for a case. */
+int tclb_batch_poll(tclb_batch_h b, int case_id, long long* iterations_done, int* remaining);
+int tclb_batch_get_globals(tclb_batch_h b, int case_id, double* out);
+int tclb_batch_get_quantity(tclb_batch_h b, int case_id, int q, void* out, double scale);
+int tclb_batch_info(tclb_batch_h b, int* ncases_active, int* ntiles, size_t* used_bytes, size_t* budget_bytes);
+/* Node updates the next step will perform (as of the last status read-back). */
+long long tclb_batch_pending_updates(tclb_batch_h b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,244 @@
+"""Runners for the benchmark configurations other than the headline one.
+
+Each returns a dict that bench.py prints as one JSON line. All inputs are
+seeded synthetic cases (tclb_b200.cases); timings use CUDA events on the
+lattice's stream or, for the batch and serving loops whose work spans several
+streams, synchronised wall-clock time around the whole run.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import time
+from typing import Dict, List
+
+import numpy as np
+
+from . import cases
+from . import models as M
+from .batch import Batch, CaseSpec, autotune
+from .lattice import Lattice
+from .serve import Request, Server
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def hbm_peak() -> float:
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def _events(torch, stream):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return a, b
+
+
+# ---------------------------------------------------------------------------
+# Configuration 1: d2q9 channel with a disc, FP64 (and FP32), 10k iterations
+# ---------------------------------------------------------------------------
+def config1(iterations: int = 10000, log_every: int = 100, precision: str = "fp64") -> dict:
+    import torch
+
+    nx, ny = 1024, 256
+    lat = Lattice("d2q9", nx, ny, precision=precision)
+    lat.set_flags(cases.channel_disc_d2q9(nx, ny, r=16, cx=256, cy=128))
+    for kind, name, v in cases.channel_disc_settings(ux=0.01, nu=0.02, bgk=True):
+        lat.set_zone_setting(name, v) if kind == "zone" else lat.SetSetting(name, v)
+    lat.Init()
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    lat.Iterate(log_every, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)  # warm-up, graph capture
+    lat.Init()
+    log = []
+    a, b = _events(torch, stream)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(iterations // log_every):
+        lat.Iterate(log_every, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        log.append(lat.globals.tolist())
+    b.record(stream)
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    mlups = lat.N * iterations / t / 1e6
+    g = lat.globals_dict()
+    u = lat.GetQuantity("U")
+    lat.close()
+    bpu = 2 * 9 * (8 if precision == "fp64" else 4) + 2
+    return {"config": "1: d2q9 channel 1024x256, disc r=16 at (256,128), Zou-He inlet Ux=0.01 / outlet rho=1, "
+                      f"BGK nu=0.02, {iterations} iterations, Globals every {log_every}",
+            "precision": precision, "MLUPS": mlups, "time_s": t,
+            "hbm_roofline_frac": mlups * 1e6 * bpu / (hbm_peak() * 1e9),
+            "note": "lattice (2 x 18.9 MB) is L2-resident: the HBM roofline is not the bound; "
+                    "plain iterations replay CUDA graphs of 32",
+            "globals_final": g, "max_u": float(np.abs(u).max()), "log_rows": len(log)}
+
+
+# ---------------------------------------------------------------------------
+# Configuration 3: d3q19 porous channel, storage precision study
+# ---------------------------------------------------------------------------
+def config3(iterations: int = 5000, storages=("fp64", "fp32", "fp16s", "bf16s"), n=(384, 192, 192)) -> dict:
+    import torch
+
+    nx, ny, nz = n
+    fl = cases.porous_channel_d3q19(nx, ny, nz, p=0.08, band=4, seed=0)
+    out = {"config": f"3: d3q19 MRT {nx}x{ny}x{nz} channel, body force Fx=1e-6, nu=0.01, Bernoulli(0.08) "
+                     f"solids (seed 0, 4-node wall band free), periodic x, walls y/z, {iterations} iterations",
+           "runs": {}}
+    ref_u, ref_g = None, None
+    for st in storages:
+        prec = "fp64" if st == "fp64" else "fp32"
+        storage = "same" if st in ("fp64", "fp32") else st
+        lat = Lattice("d3q19", nx, ny, nz, precision=prec, storage=storage)
+        lat.set_flags(fl)
+        lat.SetSetting("nu", 0.01)
+        lat.SetSetting("ForceX", 1e-6)
+        lat.Init()
+        stream = torch.cuda.Stream()
+        sp = stream.cuda_stream
+        lat.Iterate(64, M.ITER_NORM, stream=sp)  # warm-up
+        lat.Init()
+        a, b = _events(torch, stream)
+        torch.cuda.synchronize()
+        a.record(stream)
+        lat.Iterate(iterations, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        b.record(stream)
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / 1e3
+        mlups = lat.N * iterations / t / 1e6
+        u = lat.GetQuantity("U").astype(np.float64)
+        g = lat.globals_dict()
+        r = {"MLUPS": mlups, "bytes_per_update": lat.bytes_per_update,
+             "hbm_roofline_frac": mlups * 1e6 * lat.bytes_per_update / (hbm_peak() * 1e9),
+             "VOLvx": g["VOLvx"], "MaxV": g["MaxV"]}
+        if st == "fp64":
+            ref_u, ref_g = u, g
+        else:
+            r["u_rel_l2_vs_fp64"] = float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u))
+            r["flux_rel_err_vs_fp64"] = float(abs(g["VOLvx"] - ref_g["VOLvx"]) / abs(ref_g["VOLvx"]))
+        out["runs"][st] = r
+        lat.close()
+    if "fp32" in out["runs"] and "fp16s" in out["runs"]:
+        out["fp16s_speedup_vs_fp32"] = out["runs"]["fp16s"]["MLUPS"] / out["runs"]["fp32"]["MLUPS"]
+    out["reference_for_errors"] = ("the GPU FP64 path of this library, which matches the CPU FP64 oracle to "
+                                   "1e-12 in the parity tests (a CPU FP64 run of this size takes about an hour)")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Configuration 4: 512 batched d2q9 cases
+# ---------------------------------------------------------------------------
+def batch_specs(n_cases=512, seed=0, iterations=2000) -> List[CaseSpec]:
+    specs, _clamps = [], 0
+    lst, clamps = cases.batch_cases_d2q9(n_cases, seed=seed)
+    for c in lst:
+        fl = cases.disc_channel_flags(c["W"], c["H"], c["r"], c["cx"], c["cy"])
+        specs.append(CaseSpec(fl, {"Viscosity": c["nu"]}, {0: {"VelocityX": c["ux"]}, 1: {"VelocityX": c["ux"]}},
+                              iterations))
+    return specs, clamps
+
+
+def single_large_mlups(model="d2q9", shape=(1, 1024, 4096), precision="fp32", storage="same", iters=200) -> float:
+    import torch
+
+    nz, ny, nx = shape
+    lat = Lattice(model, nx, ny, nz, precision=precision, storage=storage)
+    if model == "d2q9":
+        lat.set_flags(cases.disc_channel_flags(nx, ny, ny / 8, nx / 4, ny / 2))
+        lat.SetSetting("Viscosity", 0.02)
+        lat.set_zone_setting("VelocityX", 0.02)
+    else:
+        lat.set_flags(cases.porous_channel_d3q19(nx, ny, nz, p=0.08, band=2, seed=1))
+        lat.SetSetting("nu", 0.02)
+    lat.Init()
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    lat.Iterate(64, stream=sp)
+    a, b = _events(torch, stream)
+    torch.cuda.synchronize()
+    a.record(stream)
+    lat.Iterate(iters, stream=sp)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    n = lat.N
+    lat.close()
+    return n * iters / t / 1e6
+
+
+def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True) -> dict:
+    specs, clamps = batch_specs(n_cases, iterations=iterations)
+    nodes = sum(int(np.prod(s.shape)) for s in specs)
+    out = {"config": f"4: {n_cases} d2q9 BGK-like cases, W log-uniform 64..2048 (H=W/4), one disc each, "
+                     f"Ux=0.02, Re U[20,200], {iterations} iterations each, persistent graph-captured launches",
+           "nodes_total": nodes, "omega_clamps": clamps, "runs": {}}
+    for st in storages:
+        tuned = None
+        if tune:
+            sample = specs[:: max(1, len(specs) // 64)]
+            tuned = autotune("d2q9", sample, precision="fp32", storage=st, trial_iters=64)
+        b = Batch("d2q9", "fp32", storage=st, budget_bytes=100 << 30, max_cases=n_cases)
+        if tuned:
+            b.set_launch(tuned["bx"], tuned["by"], tuned["K"])
+        t_add = time.perf_counter()
+        ids = [b.add_case(s) for s in specs]
+        t_add = time.perf_counter() - t_add
+        b.sync()
+        t0 = time.perf_counter()
+        steps = b.run_to_completion()
+        t = time.perf_counter() - t0
+        mlups = nodes * iterations / t / 1e6
+        single = single_large_mlups(storage=st)
+        r = {"MLUPS": mlups, "cases_per_s": n_cases / t, "time_s": t, "replays": steps,
+             "admission_s": t_add, "single_large_case_MLUPS": single, "fraction_of_single": mlups / single,
+             "launch": dict(zip(("bx", "by", "K"), b.get_launch()))}
+        if tuned:
+            r["autotune_table"] = tuned["table"]
+        out["runs"][st] = r
+        b.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Configuration 5: serving a Poisson stream of mixed requests
+# ---------------------------------------------------------------------------
+def serve_requests(n_requests=120, rate=6.0, seed=0, d3_edge=(64, 256), iters=(500, 5000)) -> List[Request]:
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    d2, _ = cases.batch_cases_d2q9(n_requests, seed=seed + 1)
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        n_it = int(rng.integers(iters[0], iters[1] + 1))
+        if rng.random() < 0.7:
+            c = d2[i]
+            fl = cases.disc_channel_flags(c["W"], c["H"], c["r"], c["cx"], c["cy"])
+            spec = CaseSpec(fl, {"Viscosity": c["nu"]}, {0: {"VelocityX": c["ux"]}, 1: {"VelocityX": c["ux"]}}, n_it)
+            out.append(Request(i, "d2q9", spec, t))
+        else:
+            e = int(rng.integers(d3_edge[0], d3_edge[1] + 1))
+            e = max(32, cases.pad_nx(e) if e % 32 else e)
+            p = float(rng.uniform(0.02, 0.15))
+            fl = cases.porous_channel_d3q19(e, e, e, p=p, band=2, seed=1000 + i)
+            spec = CaseSpec(fl, {"nu": 0.02, "ForceX": 1e-5}, {}, n_it)
+            out.append(Request(i, "d3q19", spec, t))
+    return out
+
+
+def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150) -> dict:
+    out = {"config": f"5: serving, Poisson arrivals (rate {rate}/s, seed 0), 70% d2q9 obstacle channels (config-4 "
+                     "sizes), 30% d3q19 porous boxes (edge U[64,256], p U[0.02,0.15]), iterations U[500,5000], "
+                     f"admission by footprint under {budget_gb} GB, resident lattices, continuous batching",
+           "runs": {}}
+    for st in storages:
+        reqs = serve_requests(n_requests, rate)
+        srv = Server(("d2q9", "d3q19"), "fp32", st, budget_bytes=budget_gb << 30,
+                     launch={"d2q9": (128, 2, 64), "d3q19": (64, 4, 16)})
+        rep = srv.run(reqs)
+        srv.close()
+        single = single_large_mlups("d3q19", (256, 256, 256), storage=st, iters=100)
+        rep["single_large_case_MLUPS_d3q19"] = single
+        rep["fraction_of_single"] = rep["busy_mlups"] / single
+        out["runs"][st] = rep
+    return out

@@ -1,0 +1,96 @@
+// Batched iteration of many independent lattices in one persistent launch.
+//
+// No counterpart in the reference: TCLB runs one lattice per process. Here
+// each case (lattice) has a device descriptor; the cases' nodes are cut into
+// uniform tiles (one thread block each) listed in a device tile table, and a
+// persistent grid walks the table with a grid stride, so uneven case sizes
+// balance across the SMs. The physics is the per-model node update of
+// lbm_kernels.cuh, unchanged.
+//
+// A launch is iteration k (0-based) of a replay of K iterations. Case c runs
+// it when k < remaining[c]; its A/B parity is (counter[c] + k) & 1. The
+// counters advance only in k_batch_advance at the end of a replay, so a CUDA
+// graph of K launches + advance can be replayed while cases come and go.
+#pragma once
+#include "lbm_kernels.cuh"
+
+namespace tclb {
+
+constexpr int BATCH_MAX_SET = 16;
+
+struct BatchCase {
+  void* buf[2];
+  const flag_t* flags;
+  const void* zone;  // real_t [zones][NZS]
+  double* glob;      // [NG] Globals of the case's last iteration in a replay
+  size_t stride;
+  int nx, ny, nz;
+  int counter;    // iterations done
+  int remaining;  // iterations left
+  int active;
+  double s[BATCH_MAX_SET];
+};
+
+struct BatchTile {
+  int slot, x0, y0, z;
+};
+
+template <class M, class R, class St>
+__global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restrict__ cases,
+                                                       const BatchTile* __restrict__ tiles,
+                                                       const int* __restrict__ ntiles_p, int k, int K) {
+  const int ntiles = *ntiles_p;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    const BatchCase& C = cases[tile.slot];
+    const int remaining = C.remaining;
+    if (!C.active || k >= remaining) continue;  // uniform across the block
+    const int last = (remaining < K ? remaining : K) - 1;
+    const int parity = (C.counter + k) & 1;
+    Args<R, M::NSET> a;
+    a.src = C.buf[parity];
+    a.dst = C.buf[1 - parity];
+    a.stride = C.stride;
+    a.flags = C.flags;
+    a.nx = C.nx;
+    a.ny = C.ny;
+    a.nz = C.nz;
+    a.zone = static_cast<const R*>(C.zone);
+    a.glob = C.glob;
+#pragma unroll
+    for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
+    const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
+    const bool act = x < a.nx && y < a.ny;
+    if (k == last) {
+      R g[M::NG];
+#pragma unroll
+      for (int i = 0; i < M::NG; i++) g[i] = 0;
+      if (act) node_update<M, R, St, true>(a, x, y, z, g);
+      reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+      __syncthreads();  // shared scratch of reduce_globals reused by the next tile
+    } else if (act) {
+      R g[1];
+      node_update<M, R, St, false>(a, x, y, z, g);
+    }
+  }
+}
+
+// End of a replay: counters and remaining iterations of every active case.
+__global__ void k_batch_advance(BatchCase* cases, int ncases, int K) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases || !cases[c].active) return;
+  const int r = cases[c].remaining;
+  const int d = r < K ? r : K;
+  cases[c].counter += d;
+  cases[c].remaining = r - d;
+}
+
+// Clear the Globals of every case at the start of a replay.
+template <int NG>
+__global__ void k_batch_clear_globals(BatchCase* cases, int ncases) {
+  const int c = blockIdx.x;
+  if (c >= ncases || !cases[c].active || cases[c].remaining <= 0) return;
+  for (int i = threadIdx.x; i < NG; i += blockDim.x) cases[c].glob[i] = 0.0;
+}
+
+}  // namespace tclb

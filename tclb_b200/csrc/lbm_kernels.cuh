@@ -325,6 +325,16 @@ struct D3Q19 {
     f[13] = f[12] + rho * ux / R(6) + Nxz;
   }
 
+  // <plane>vx, vy, vz, rho, area of one slice (:271-279)
+  template <int B, class R>
+  __device__ __forceinline__ static void plane(R* g, R ux, R uy, R uz, R rs, const R* zs) {
+    glob(g, B + 0, ux, zs);
+    glob(g, B + 1, uy, zs);
+    glob(g, B + 2, uz, zs);
+    glob(g, B + 3, rs, zs);
+    glob(g, B + 4, R(1), zs);
+  }
+
   template <class R, bool G>
   __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
     R m[Q];
@@ -377,14 +387,11 @@ struct D3Q19 {
     d3q19_populations(m, f);
     if (G) {  // :266-289, with rho and J already divided by Mw (C(R, Mw, eq="/="))
       const R rs = m[0], ux = m[3] / rs, uy = m[5] / rs, uz = m[7] / rs;
-      const unsigned pl = fl & d3q19::ADDITIONALS;
-      if (pl) {
-        const int b = 1 + 5 * (int)(pl - 1);
-        glob(g, b + 0, ux, zs);
-        glob(g, b + 1, uy, zs);
-        glob(g, b + 2, uz, zs);
-        glob(g, b + 3, rs, zs);
-        glob(g, b + 4, R(1), zs);
+      switch (fl & d3q19::ADDITIONALS) {  // constant indices keep g[] in registers
+        case d3q19::XYslice: plane<d3q19::G_XY>(g, ux, uy, uz, rs, zs); break;
+        case d3q19::XZslice: plane<d3q19::G_XZ>(g, ux, uy, uz, rs, zs); break;
+        case d3q19::YZslice: plane<d3q19::G_YZ>(g, ux, uy, uz, rs, zs); break;
+        default: break;
       }
       glob(g, d3q19::G_VOLvx, ux, zs);
       glob(g, d3q19::G_VOLvy, uy, zs);
@@ -610,19 +617,6 @@ struct D3Q27C {
   template <class R, bool G>
   __device__ __forceinline__ static void collide(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
     const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
-    if (G) {  // :311-319, getU_ :30-45
-      R rho = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-      for (int i = 0; i < Q; i++) { rho += f[i]; jx += R(ex(i)) * f[i]; jy += R(ey(i)) * f[i]; jz += R(ez(i)) * f[i]; }
-      R ux = (jx + Fx / R(2)) / rho, uy = (jy + Fy / R(2)) / rho, uz = (jz + Fz / R(2)) / rho;
-      if ((fl & d3q27c::BOUNDARY) == d3q27c::Wall) ux = uy = uz = 0;
-      glob(g, d3q27c::G_Density, rho, zs);
-      glob(g, d3q27c::G_Flux, ux, zs);
-      glob(g, d3q27c::G_Mass, rho, zs);
-      glob(g, d3q27c::G_XMomentum, rho * ux, zs);
-      glob(g, d3q27c::G_YMomentum, rho * uy, zs);
-      glob(g, d3q27c::G_ZMomentum, rho * uz, zs);
-    }
     const R w0 = (fl & d3q27c::BOUNDARY) ? R(1) / (R(3) * a.s[d3q27c::S_nubuffer] + R(0.5))
                                          : R(1) / (R(3) * a.s[d3q27c::S_nu] + R(0.5));
     const R w1 = R(1);
@@ -635,6 +629,17 @@ struct D3Q27C {
       for (int x = 0; x < 3; x++) raw3(f[x + 9 * c], f[x + 3 + 9 * c], f[x + 6 + 9 * c]);
 #pragma unroll
     for (int r = 0; r < 9; r++) raw3(f[r], f[r + 9], f[r + 18]);
+    if (G) {  // :311-319 with getU_ (:30-45); rho and J are the raw moments m000, m100, m010, m001
+      const R rho = f[0], jx = f[1], jy = f[3], jz = f[9];
+      R ux = (jx + Fx / R(2)) / rho, uy = (jy + Fy / R(2)) / rho, uz = (jz + Fz / R(2)) / rho;
+      if ((fl & d3q27c::BOUNDARY) == d3q27c::Wall) ux = uy = uz = 0;
+      glob(g, d3q27c::G_Density, rho, zs);
+      glob(g, d3q27c::G_Flux, ux, zs);
+      glob(g, d3q27c::G_Mass, rho, zs);
+      glob(g, d3q27c::G_XMomentum, rho * ux, zs);
+      glob(g, d3q27c::G_YMomentum, rho * uy, zs);
+      glob(g, d3q27c::G_ZMomentum, rho * uz, zs);
+    }
     R c[Q];
     const R m0 = f[0], im0 = R(1) / m0;
     cum_from_raw(f, c, im0);
@@ -761,39 +766,41 @@ __device__ __forceinline__ void reduce_globals(const R (&g)[NG], double* out) {
 // ---------------------------------------------------------------------------
 // The fused iteration kernel: one thread per node.
 // ---------------------------------------------------------------------------
+// One node: pull from a.src with periodic wrap, run the model, store to a.dst.
+template <class M, class R, class St, bool G>
+__device__ __forceinline__ void node_update(const Args<R, M::NSET>& a, int x, int y, int z, R* g) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
+  const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
+  const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
+  const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src);
+  typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst);
+  const int node = x + nx * (y + ny * z);
+  const flag_t fl = a.flags[node];
+  R f[M::Q];
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) {
+    const int sx = M::ex(i) == 0 ? x : (M::ex(i) > 0 ? xm : xp);
+    const int sy = M::ey(i) == 0 ? y : (M::ey(i) > 0 ? ym : yp);
+    const int sz = M::DIM == 2 ? z : (M::ez(i) == 0 ? z : (M::ez(i) > 0 ? zm : zp));
+    f[i] = St::template load<R>(src + (size_t)i * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(i)));
+  }
+  M::template run<R, G>(f, fl, a, g);
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
+}
+
 template <class M, class R, class St, bool G>
 __global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   const bool act = (x < a.nx) && (y < a.ny);
-  R g[M::NG];
-  if (G) {
+  R g[G ? M::NG : 1];
 #pragma unroll
-    for (int i = 0; i < M::NG; i++) g[i] = 0;
-  }
-  if (act) {
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
-    const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
-    const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
-    const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src);
-    typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst);
-    const int node = x + nx * (y + ny * z);
-    const flag_t fl = a.flags[node];
-    R f[M::Q];
-#pragma unroll
-    for (int i = 0; i < M::Q; i++) {
-      const int sx = M::ex(i) == 0 ? x : (M::ex(i) > 0 ? xm : xp);
-      const int sy = M::ey(i) == 0 ? y : (M::ey(i) > 0 ? ym : yp);
-      const int sz = M::DIM == 2 ? z : (M::ez(i) == 0 ? z : (M::ez(i) > 0 ? zm : zp));
-      f[i] = St::template load<R>(src + (size_t)i * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(i)));
-    }
-    M::template run<R, G>(f, fl, a, g);
-#pragma unroll
-    for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
-  }
-  if (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+  for (int i = 0; i < (G ? M::NG : 1); i++) g[i] = 0;
+  if (act) node_update<M, R, St, G>(a, x, y, z, g);
+  if constexpr (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
 }
 
 // BaseInit stage: equilibrium from settings, written to the current snapshot.

@@ -144,6 +144,10 @@ struct tclb_lattice {
   void* qbuf = nullptr;
   size_t qbuf_bytes = 0;
   const Impl* impl = nullptr;
+  // CUDA graphs of GRAPH_CHUNK plain iterations starting from snapshot 0 / 1;
+  // settings travel as kernel parameters, so a settings change drops them.
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int use_graphs = 1;
 };
 
 struct Impl {
@@ -255,6 +259,43 @@ int upload_zone(tclb_lattice* L) {
     return TCLB_OK;
   }
   TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
+constexpr int GRAPH_CHUNK = 32;
+
+void drop_graphs(tclb_lattice* L) {
+  for (int p = 0; p < 2; p++)
+    if (L->graph[p]) {
+      cudaGraphExecDestroy(L->graph[p]);
+      L->graph[p] = nullptr;
+    }
+}
+
+// Capture GRAPH_CHUNK plain iterations starting from the current snapshot.
+int ensure_iter_graph(tclb_lattice* L, cudaStream_t s) {
+  const int p = L->cur;
+  if (L->graph[p]) return TCLB_OK;
+  cudaStream_t cs;
+  TCLB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int k = 0; k < GRAPH_CHUNK; k++) {
+      L->impl->iterate(L, false, cs);
+      L->cur = 1 - L->cur;
+    }
+    e = cudaStreamEndCapture(cs, &g);
+  }
+  L->cur = p;  // capture recorded the launches without running them
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&L->graph[p], g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    L->graph[p] = nullptr;
+    return fail(TCLB_ERR_CUDA, std::string("iteration graph: ") + cudaGetErrorString(e));
+  }
+  (void)s;
   return TCLB_OK;
 }
 
@@ -396,6 +437,7 @@ int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, i
 int tclb_destroy(tclb_h L) {
   CHECK_H(L);
   cudaStreamSynchronize(L->stream);
+  drop_graphs(L);
   if (L->qbuf) cudaFree(L->qbuf);
   cudaFree(L->pool);
   cudaStreamDestroy(L->stream);
@@ -440,6 +482,7 @@ int tclb_get_flags(tclb_h L, uint16_t* flags) {
 int tclb_set_setting(tclb_h L, int i, double v) {
   CHECK_H(L);
   if (i < 0 || i >= L->T->nsettings) return fail(TCLB_ERR_ARG, "setting index out of range");
+  drop_graphs(L);
   return set_setting_rec(L, i, v, 0);
 }
 
@@ -507,7 +550,20 @@ int tclb_iterate(tclb_h L, int niter, int iter_type, void* stream) {
   const bool integ = (iter_type & TCLB_ITER_INTEG) == TCLB_ITER_INTEG;
   if (integ) last_glob = 0;
   bool globs = (iter_type & TCLB_ITER_GLOBS) != 0;
-  for (int i = 0; i < niter; i++) {
+  int i = 0;
+  if (!globs && L->use_graphs) {
+    // plain iterations in graph replays of GRAPH_CHUNK (even: the snapshot
+    // parity is unchanged by a replay)
+    const int plain = niter - (last_glob ? 1 : 0);
+    while (plain - i >= GRAPH_CHUNK) {
+      int rc = ensure_iter_graph(L, s);
+      if (rc) return rc;
+      TCLB_CK(cudaGraphLaunch(L->graph[L->cur], s));
+      i += GRAPH_CHUNK;
+      L->iter += GRAPH_CHUNK;
+    }
+  }
+  for (; i < niter; i++) {
     if (last_glob && i == niter - 1) {
       TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, L->T->nglobals * sizeof(double), s));
       globs = true;
@@ -627,6 +683,16 @@ int tclb_get_iteration(tclb_h L, long long* iter) {
 }
 
 double tclb_bytes_per_update(tclb_h L) { return L ? 2.0 * L->T->Q * L->elem + sizeof(flag_t) : 0.0; }
+
+int tclb_set_launch(tclb_h L, int bx, int by, int use_graphs) {
+  CHECK_H(L);
+  if (bx < 32 || bx % 32 || by < 1 || bx * by > 256) return fail(TCLB_ERR_ARG, "bad block shape");
+  drop_graphs(L);
+  L->bx = bx;
+  L->by = by;
+  L->use_graphs = use_graphs ? 1 : 0;
+  return TCLB_OK;
+}
 
 int tclb_sync(tclb_h L) {
   CHECK_H(L);

@@ -71,6 +71,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_bytes_per_update.argtypes = [h]
     L.tclb_bytes_per_update.restype = d
     L.tclb_sync.argtypes = [h]
+    L.tclb_set_launch.argtypes = [h, i, i, i]
     _lib = L
     return L
 
@@ -239,3 +240,6 @@ class Lattice:
 
     def sync(self):
         _check(self.lib.tclb_sync(self._h))
+
+    def set_launch(self, bx: int, by: int, use_graphs: bool = True):
+        _check(self.lib.tclb_set_launch(self._h, int(bx), int(by), 1 if use_graphs else 0))

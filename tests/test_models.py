@@ -90,3 +90,13 @@ def test_library_exports_header_symbols():
     lib = load_library()
     for n in sorted(names):
         assert hasattr(lib, n), n
+
+
+def test_batch_case_footprint():
+    from tclb_b200.batch import case_bytes
+
+    # d2q9 FP32 128x32: 2 snapshots of 9 planes (256-byte aligned) + flags + zone table + Globals
+    n = 128 * 32
+    expect = 2 * 9 * n * 4 + n * 2 + 512 * 6 * 4 + 256
+    assert case_bytes("d2q9", 128, 32) == expect
+    assert case_bytes("d3q19", 64, 64, 64, storage="fp16s") > 2 * 19 * 64 ** 3 * 2
