@@ -7,6 +7,11 @@
 // balance across the SMs. The physics is the per-model node update of
 // lbm_kernels.cuh, unchanged.
 //
+// A tile is a run of bx*by consecutive nodes of one case (x fastest), so
+// narrow cases leave no thread idle except in their last tile; nx is a
+// multiple of 32 after TCLB's padding, so every warp stays inside one row and
+// the loads stay coalesced.
+//
 // A launch is iteration k (0-based) of a replay of K iterations. Case c runs
 // it when k < remaining[c]; its A/B parity is (counter[c] + k) & 1. The
 // counters advance only in k_batch_advance at the end of a replay, so a CUDA
@@ -32,7 +37,7 @@ struct BatchCase {
 };
 
 struct BatchTile {
-  int slot, x0, y0, z;
+  int slot, start;  // first node (linear index) of the tile
 };
 
 template <class M, class R, class St>
@@ -59,8 +64,10 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
     a.glob = C.glob;
 #pragma unroll
     for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
-    const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
-    const bool act = x < a.nx && y < a.ny;
+    const int n = tile.start + threadIdx.x + blockDim.x * threadIdx.y;
+    const int sxy = a.nx * a.ny;
+    const bool act = n < sxy * a.nz;
+    const int z = n / sxy, r = n - z * sxy, y = r / a.nx, x = r - y * a.nx;
     if (k == last) {
       R g[M::NG];
 #pragma unroll

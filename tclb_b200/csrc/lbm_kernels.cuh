@@ -767,27 +767,35 @@ __device__ __forceinline__ void reduce_globals(const R (&g)[NG], double* out) {
 // The fused iteration kernel: one thread per node.
 // ---------------------------------------------------------------------------
 // One node: pull from a.src with periodic wrap, run the model, store to a.dst.
+//
+// Addressing: the source of population i is node - e_i with periodic wrap.
+// Per axis the two possible offsets (pulling from the lower / upper
+// neighbour, wrapped at the faces) are computed once; each population's
+// offset is then the sum of three of them, chosen at compile time, and the
+// population planes are reached by adding the plane stride to one pointer.
 template <class M, class R, class St, bool G>
 __device__ __forceinline__ void node_update(const Args<R, M::NSET>& a, int x, int y, int z, R* g) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
-  const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
-  const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
-  const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src);
-  typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst);
-  const int node = x + nx * (y + ny * z);
+  const int sxy = nx * ny;
+  const int node = x + nx * y + sxy * z;
+  const int ox_lo = x == 0 ? nx - 1 : -1, ox_hi = x + 1 == nx ? 1 - nx : 1;                // e_x = +1 / -1
+  const int oy_lo = y == 0 ? nx * (ny - 1) : -nx, oy_hi = y + 1 == ny ? nx * (1 - ny) : nx;  // e_y = +1 / -1
+  const int oz_lo = z == 0 ? sxy * (nz - 1) : -sxy, oz_hi = z + 1 == nz ? sxy * (1 - nz) : sxy;
+  const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src) + node;
+  typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst) + node;
+  const size_t stride = a.stride;
   const flag_t fl = a.flags[node];
   R f[M::Q];
 #pragma unroll
   for (int i = 0; i < M::Q; i++) {
-    const int sx = M::ex(i) == 0 ? x : (M::ex(i) > 0 ? xm : xp);
-    const int sy = M::ey(i) == 0 ? y : (M::ey(i) > 0 ? ym : yp);
-    const int sz = M::DIM == 2 ? z : (M::ez(i) == 0 ? z : (M::ez(i) > 0 ? zm : zp));
-    f[i] = St::template load<R>(src + (size_t)i * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(i)));
+    const int o = (M::ex(i) > 0 ? ox_lo : (M::ex(i) < 0 ? ox_hi : 0)) +
+                  (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0)) +
+                  (M::DIM == 2 ? 0 : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0)));
+    f[i] = St::template load<R>(src + i * stride + o, R(M::w(i)));
   }
   M::template run<R, G>(f, fl, a, g);
 #pragma unroll
-  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + (size_t)i * a.stride + node, f[i], R(M::w(i)));
+  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + i * stride, f[i], R(M::w(i)));
 }
 
 template <class M, class R, class St, bool G>
