@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtclb_b200.so")
 SOURCES = ["tclb_b200.cu", "batch.cu"]
-HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "tclb_models.h", "cumulant_gen.cuh", "d3q19_gen.cuh"]
+HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "tclb_models.h", "cumulant_gen.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -268,7 +268,7 @@ struct D2Q9 {
 // ---------------------------------------------------------------------------
 // d3q19 (models/flow/d3q19/Dynamics.c.Rt)
 // ---------------------------------------------------------------------------
-#include "d3q19_gen.cuh"
+
 
 struct D3Q19 {
   static constexpr int Q = 19, DIM = 3, NSET = d3q19::NSET, NZS = d3q19::NZS, NG = d3q19::NG, NSUM = d3q19::NSUM,
@@ -335,58 +335,88 @@ struct D3Q19 {
     glob(g, B + 4, R(1), zs);
   }
 
+  // Pairs (i, opposite of i); pair p has direction e of its first member.
+  __host__ __device__ static constexpr int pair_a(int p) { return p < 3 ? 1 + 2 * p : (p < 5 ? 4 + p : (p < 7 ? 6 + p : 8 + p)); }
+  __host__ __device__ static constexpr int pair_b(int p) { return opp(pair_a(p)); }
+
+  // TCLB's d3q19 equilibrium (Req . MRTMAT^-1, lib/d3q19.R:40-62) split into
+  // the part even under e -> -e (e[p], e0 for the rest population) and the
+  // odd part o[p] of the first member of each pair. With X = Jx^2/rho etc.:
+  //   rest:        rho/3 - (X+Y+Z)/3
+  //   +-x axis:    rho/18 + X/6 - (Y+Z)/6     +-  Jx/6
+  //   (sx,sy,0):   rho/36 + (X+Y)/12 + sx*sy*Jx*Jy/(4 rho)  +  (sx*Jx + sy*Jy)/12
+  // (and the same with the axes permuted).
+  template <class R>
+  __device__ __forceinline__ static void feq_parts(R rho, R irho, R jx, R jy, R jz, R& e0, R (&e)[9], R (&o)[9]) {
+    const R X = jx * jx * irho, Y = jy * jy * irho, Z = jz * jz * irho;
+    const R c18 = rho * R(1.0 / 18.0), c36 = rho * R(1.0 / 36.0);
+    e0 = (rho - X - Y - Z) * R(1.0 / 3.0);
+    e[0] = c18 + (X - Y - Z) * R(1.0 / 6.0);
+    e[1] = c18 + (Y - X - Z) * R(1.0 / 6.0);
+    e[2] = c18 + (Z - X - Y) * R(1.0 / 6.0);
+    const R xy = c36 + (X + Y) * R(1.0 / 12.0), pxy = R(0.25) * jx * jy * irho;
+    const R xz = c36 + (X + Z) * R(1.0 / 12.0), pxz = R(0.25) * jx * jz * irho;
+    const R yz = c36 + (Y + Z) * R(1.0 / 12.0), pyz = R(0.25) * jy * jz * irho;
+    e[3] = xy + pxy;  // 7 (1,1,0)
+    e[4] = xy - pxy;  // 8 (-1,1,0)
+    e[5] = xz + pxz;  // 11 (1,0,1)
+    e[6] = xz - pxz;  // 12 (-1,0,1)
+    e[7] = yz + pyz;  // 15 (0,1,1)
+    e[8] = yz - pyz;  // 16 (0,-1,1)
+    o[0] = jx * R(1.0 / 6.0);
+    o[1] = jy * R(1.0 / 6.0);
+    o[2] = jz * R(1.0 / 6.0);
+    o[3] = (jx + jy) * R(1.0 / 12.0);
+    o[4] = (jy - jx) * R(1.0 / 12.0);
+    o[5] = (jx + jz) * R(1.0 / 12.0);
+    o[6] = (jz - jx) * R(1.0 / 12.0);
+    o[7] = (jy + jz) * R(1.0 / 12.0);
+    o[8] = (jz - jy) * R(1.0 / 12.0);
+  }
+
+  // CollisionMRT (:223-290). The d'Humieres rates of TCLB's d3q19 give every
+  // non-conserved moment that is even under e -> -e the rate gamma1 = 1-omega
+  // and every non-conserved odd moment gamma2 = 1 - 8(2-omega)/(8-omega);
+  // the conserved ones are rho (even) and J (odd). The moment-space update
+  //   R <- S (R - Req(J)) + Req(J + rho F),  f = R . MRTMAT^-1
+  // is therefore the same linear map as, in population space,
+  //   f_i <- feq_i(J') + gamma1 (f - feq(J))_i^even + gamma2 (f - feq(J))_i^odd
+  // with even/odd parts taken over each pair (i, opposite i). It is evaluated
+  // that way here: pair sums and differences instead of two 19x19 transforms.
   template <class R, bool G>
   __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
-    R m[Q];
-    d3q19_moments(f, m);
+    R s[9], d[9];
+#pragma unroll
+    for (int p = 0; p < 9; p++) {
+      s[p] = f[pair_a(p)] + f[pair_b(p)];
+      d[p] = f[pair_a(p)] - f[pair_b(p)];
+    }
+    const R rho = f[0] + (s[0] + s[1] + s[2]) + ((s[3] + s[4]) + (s[5] + s[6]) + (s[7] + s[8]));
+    R jx = d[0] + d[3] - d[4] + d[5] - d[6];
+    R jy = d[1] + d[3] + d[4] + d[7] - d[8];
+    R jz = d[2] + d[5] + d[6] + d[7] + d[8];
     const R omega = a.s[d3q19::S_omega];
     const R g1 = R(1) - omega;
     const R g2 = R(1) - R(8) * (R(2) - omega) / (R(8) - omega);
-    const R rho = m[0], irho = R(1) / rho;
-    R jx = m[3], jy = m[5], jz = m[7];
-    // equilibrium moments of TCLB's d3q19 (lib/d3q19.R:40-62), 0-based index
-    auto req = [&](R Jx, R Jy, R Jz, R (&q)[Q]) {
-      const R j2 = (Jx * Jx + Jy * Jy + Jz * Jz) * irho;
-      const R pxx = (R(2) * Jx * Jx - Jy * Jy - Jz * Jz) * irho;
-      const R pww = (Jy * Jy - Jz * Jz) * irho;
-      q[1] = R(-11) * rho + R(19) * j2;
-      q[2] = R(3) * rho - R(2) * j2;
-      q[4] = R(-2.0 / 3.0) * Jx;
-      q[6] = R(-2.0 / 3.0) * Jy;
-      q[8] = R(-2.0 / 3.0) * Jz;
-      q[9] = pxx;
-      q[10] = -pxx;
-      q[11] = pww;
-      q[12] = -pww;
-      q[13] = Jx * Jy * irho;
-      q[14] = Jy * Jz * irho;
-      q[15] = Jx * Jz * irho;
-      q[16] = 0; q[17] = 0; q[18] = 0;
-    };
-    R q[Q];
-    req(jx, jy, jz, q);
-#pragma unroll
-    for (int k = 0; k < Q; k++) {
-      if (k == 0 || k == 3 || k == 5 || k == 7) continue;
-      const R s = (k == 1 || k == 2 || (k >= 9 && k <= 15)) ? g1 : g2;
-      m[k] = s * (m[k] - q[k]);
-    }
+    const R irho = R(1) / rho;
+    R e0, e[9], o[9];
+    feq_parts(rho, irho, jx, jy, jz, e0, e, o);
     jx += rho * a.s[d3q19::S_ForceX];
     jy += rho * a.s[d3q19::S_ForceY];
     jz += rho * a.s[d3q19::S_ForceZ];
-    req(jx, jy, jz, q);
+    R e0n, en[9], on[9];
+    feq_parts(rho, irho, jx, jy, jz, e0n, en, on);
+    f[0] = e0n + g1 * (f[0] - e0);
 #pragma unroll
-    for (int k = 0; k < Q; k++) {
-      if (k == 0 || k == 3 || k == 5 || k == 7) continue;
-      m[k] += q[k];
+    for (int p = 0; p < 9; p++) {
+      const R E = en[p] + g1 * (R(0.5) * s[p] - e[p]);
+      const R O = on[p] + g2 * (R(0.5) * d[p] - o[p]);
+      f[pair_a(p)] = E + O;
+      f[pair_b(p)] = E - O;
     }
-    m[3] = jx; m[5] = jy; m[7] = jz;
-    const double mw[Q] = D3Q19_MW;
-#pragma unroll
-    for (int k = 0; k < Q; k++) m[k] *= R(1.0 / mw[k]);
-    d3q19_populations(m, f);
-    if (G) {  // :266-289, with rho and J already divided by Mw (C(R, Mw, eq="/="))
-      const R rs = m[0], ux = m[3] / rs, uy = m[5] / rs, uz = m[7] / rs;
+    if (G) {  // :266-289, with rho and J already divided by Mw = 19, 10 (C(R, Mw, eq="/="))
+      const R rs = rho * R(1.0 / 19.0), px = jx * R(0.1), py = jy * R(0.1), pz = jz * R(0.1);
+      const R ux = px / rs, uy = py / rs, uz = pz / rs;
       switch (fl & d3q19::ADDITIONALS) {  // constant indices keep g[] in registers
         case d3q19::XYslice: plane<d3q19::G_XY>(g, ux, uy, uz, rs, zs); break;
         case d3q19::XZslice: plane<d3q19::G_XZ>(g, ux, uy, uz, rs, zs); break;
@@ -396,9 +426,9 @@ struct D3Q19 {
       glob(g, d3q19::G_VOLvx, ux, zs);
       glob(g, d3q19::G_VOLvy, uy, zs);
       glob(g, d3q19::G_VOLvz, uz, zs);
-      glob(g, d3q19::G_VOLpx, m[3], zs);
-      glob(g, d3q19::G_VOLpy, m[5], zs);
-      glob(g, d3q19::G_VOLpz, m[7], zs);
+      glob(g, d3q19::G_VOLpx, px, zs);
+      glob(g, d3q19::G_VOLpy, py, zs);
+      glob(g, d3q19::G_VOLpz, pz, zs);
       glob(g, d3q19::G_VOLrho, rs, zs);
       glob(g, d3q19::G_VOLvolume, R(1), zs);
       const R v = sqrt(ux * ux + uy * uy + uz * uz);
@@ -462,20 +492,14 @@ struct D3Q19 {
   // SetEquilibrum (:212-217): f = Req(rho, J) . MRTMAT.inv
   template <class R>
   __device__ __forceinline__ static void equilibrium(R (&f)[Q], R rho, R jx, R jy, R jz) {
-    const R irho = R(1) / rho;
-    const R j2 = (jx * jx + jy * jy + jz * jz) * irho;
-    const R pxx = (R(2) * jx * jx - jy * jy - jz * jz) * irho;
-    const R pww = (jy * jy - jz * jz) * irho;
-    R m[Q];
-    m[0] = rho; m[1] = R(-11) * rho + R(19) * j2; m[2] = R(3) * rho - R(2) * j2;
-    m[3] = jx; m[4] = R(-2.0 / 3.0) * jx; m[5] = jy; m[6] = R(-2.0 / 3.0) * jy; m[7] = jz; m[8] = R(-2.0 / 3.0) * jz;
-    m[9] = pxx; m[10] = -pxx; m[11] = pww; m[12] = -pww;
-    m[13] = jx * jy * irho; m[14] = jy * jz * irho; m[15] = jx * jz * irho;
-    m[16] = 0; m[17] = 0; m[18] = 0;
-    const double mw[Q] = D3Q19_MW;
+    R e0, e[9], o[9];
+    feq_parts(rho, R(1) / rho, jx, jy, jz, e0, e, o);
+    f[0] = e0;
 #pragma unroll
-    for (int k = 0; k < Q; k++) m[k] *= R(1.0 / mw[k]);
-    d3q19_populations(m, f);
+    for (int p = 0; p < 9; p++) {
+      f[pair_a(p)] = e[p] + o[p];
+      f[pair_b(p)] = e[p] - o[p];
+    }
   }
 
   template <class R>
@@ -619,7 +643,6 @@ struct D3Q27C {
     const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
     const R w0 = (fl & d3q27c::BOUNDARY) ? R(1) / (R(3) * a.s[d3q27c::S_nubuffer] + R(0.5))
                                          : R(1) / (R(3) * a.s[d3q27c::S_nu] + R(0.5));
-    const R w1 = R(1);
     // raw moments: x, y, z passes
 #pragma unroll
     for (int r = 0; r < 27; r += 3) raw3(f[r], f[r + 1], f[r + 2]);
@@ -640,9 +663,31 @@ struct D3Q27C {
       glob(g, d3q27c::G_YMomentum, rho * uy, zs);
       glob(g, d3q27c::G_ZMomentum, rho * uz, zs);
     }
+    // Cumulants of order >= 4 are set to zero by the collision and those of
+    // order 3 are scaled by (1 - Omega): with the default Omega = 1 they vanish
+    // too, so only orders <= 2 are converted (a branch uniform over the launch).
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<R, false>(f, a, w0);
+    else relax<R, true>(f, a, w0);
+    // back to populations: x, y, z passes
+#pragma unroll
+    for (int r = 0; r < 27; r += 3) unraw3(f[r], f[r + 1], f[r + 2]);
+#pragma unroll
+    for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) unraw3(f[x + 9 * cc], f[x + 3 + 9 * cc], f[x + 6 + 9 * cc]);
+#pragma unroll
+    for (int r = 0; r < 9; r++) unraw3(f[r], f[r + 9], f[r + 18]);
+  }
+
+  // Raw moments f -> cumulants -> relaxed cumulants -> raw moments (:359-477).
+  template <class R, bool THIRD>
+  __device__ __forceinline__ static void relax(R (&f)[Q], const Args<R, NSET>& a, R w0) {
+    const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
+    const R w1 = R(1);
     R c[Q];
     const R m0 = f[0], im0 = R(1) / m0;
-    cum_from_raw(f, c, im0);
+    if (THIRD) cum_from_raw_o3(f, c, im0);
+    else cum_from_raw_o2(f, c, im0);
     // relaxation (:386-449)
     const R ux = c[1] + Fx * R(0.5) * im0, uy = c[3] + Fy * R(0.5) * im0, uz = c[9] + Fz * R(0.5) * im0;
     const R c200 = c[2], c020 = c[6], c002 = c[18];
@@ -665,23 +710,15 @@ struct D3Q27C {
     c[4] *= (R(1) - w0);
     c[12] *= (R(1) - w0);
     c[10] *= (R(1) - w0);
-    const R om3 = R(1) - a.s[d3q27c::S_Omega];
+    if (THIRD) {
+      const R om3 = R(1) - a.s[d3q27c::S_Omega];
 #pragma unroll
-    for (int n = 1; n < Q; n++) {
-      const int s = n % 3 + (n / 3) % 3 + n / 9;
-      if (s == 3) c[n] = om3 * c[n];
-      if (s > 3) c[n] = 0;
+      for (int n = 1; n < Q; n++)
+        if (n % 3 + (n / 3) % 3 + n / 9 == 3) c[n] = om3 * c[n];
+      raw_from_cum_o3(c, f, m0);
+    } else {
+      raw_from_cum_o2(c, f, m0);
     }
-    raw_from_cum(c, f, m0);
-    // back to populations: x, y, z passes
-#pragma unroll
-    for (int r = 0; r < 27; r += 3) unraw3(f[r], f[r + 1], f[r + 2]);
-#pragma unroll
-    for (int cc = 0; cc < 3; cc++)
-#pragma unroll
-      for (int x = 0; x < 3; x++) unraw3(f[x + 9 * cc], f[x + 3 + 9 * cc], f[x + 6 + 9 * cc]);
-#pragma unroll
-    for (int r = 0; r < 9; r++) unraw3(f[r], f[r + 9], f[r + 18]);
   }
 
   template <class R, bool G>
