@@ -148,8 +148,12 @@ double tclb_bytes_per_update(tclb_h h);
 int tclb_sync(tclb_h h);
 
 /* Launch shape of the iteration kernel (bx multiple of 32, bx*by <= 256) and
-   whether runs of plain iterations replay a captured CUDA graph (default on). */
-int tclb_set_launch(tclb_h h, int bx, int by, int use_graphs);
+   flags: TCLB_LAUNCH_GRAPHS replays runs of plain iterations from a captured
+   CUDA graph; TCLB_LAUNCH_PAIRS lets 16-bit storage with nx % 64 == 0 update
+   two nodes per thread with 32-bit accesses. Both are on by default. */
+#define TCLB_LAUNCH_GRAPHS 1
+#define TCLB_LAUNCH_PAIRS 2
+int tclb_set_launch(tclb_h h, int bx, int by, int flags);
 
 /* ---------------------------------------------------------------------------
    Batches: many independent cases of one model advanced together by one

@@ -173,8 +173,9 @@ int rebuild_tiles(tclb_batch* B) {
   for (size_t s = 0; s < B->cases.size(); s++) {
     const BatchCase& C = B->cases[s];
     if (!B->used_slot[s] || !C.active || B->h_status[s].y <= 0) continue;  // finished cases get no tiles
-    const int N = C.nx * C.ny * C.nz, T = B->bx * B->by;
-    for (int start = 0; start < N; start += T) t.push_back({(int)s, start});
+    for (int z = 0; z < C.nz; z++)
+      for (int y = 0; y < C.ny; y += B->by)
+        for (int x = 0; x < C.nx; x += B->bx) t.push_back({(int)s, x, y, z});
   }
   if (t.size() > B->tiles_cap) {
     if (B->d_tiles) BCK(cudaFreeAsync(B->d_tiles, B->stream));

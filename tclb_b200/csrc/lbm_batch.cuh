@@ -7,10 +7,9 @@
 // balance across the SMs. The physics is the per-model node update of
 // lbm_kernels.cuh, unchanged.
 //
-// A tile is a run of bx*by consecutive nodes of one case (x fastest), so
-// narrow cases leave no thread idle except in their last tile; nx is a
-// multiple of 32 after TCLB's padding, so every warp stays inside one row and
-// the loads stay coalesced.
+// A tile is a bx x by block of nodes of one z plane of one case. With nx a
+// multiple of 32 (TCLB's padding) a tile width of 32 leaves no thread idle on
+// any case; wider tiles trade that for fewer tiles. The autotuner chooses.
 //
 // A launch is iteration k (0-based) of a replay of K iterations. Case c runs
 // it when k < remaining[c]; its A/B parity is (counter[c] + k) & 1. The
@@ -37,7 +36,7 @@ struct BatchCase {
 };
 
 struct BatchTile {
-  int slot, start;  // first node (linear index) of the tile
+  int slot, x0, y0, z;
 };
 
 template <class M, class R, class St>
@@ -45,39 +44,51 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
                                                        const BatchTile* __restrict__ tiles,
                                                        const int* __restrict__ ntiles_p, int k, int K) {
   const int ntiles = *ntiles_p;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const BatchTile tile = tiles[t];
-    const BatchCase& C = cases[tile.slot];
-    const int remaining = C.remaining;
-    if (!C.active || k >= remaining) continue;  // uniform across the block
-    const int last = (remaining < K ? remaining : K) - 1;
-    const int parity = (C.counter + k) & 1;
-    Args<R, M::NSET> a;
-    a.src = C.buf[parity];
-    a.dst = C.buf[1 - parity];
-    a.stride = C.stride;
-    a.flags = C.flags;
-    a.nx = C.nx;
-    a.ny = C.ny;
-    a.nz = C.nz;
-    a.zone = static_cast<const R*>(C.zone);
-    a.glob = C.glob;
+  // Chunks of TILE_CHUNK consecutive tiles (usually one case) walked with a
+  // grid stride: the case descriptor is read once per chunk and case.
+  constexpr int TILE_CHUNK = 4;
+  const int nchunks = (ntiles + TILE_CHUNK - 1) / TILE_CHUNK;
+  int slot = -1;
+  bool skip = true;
+  int last = 0;
+  Args<R, M::NSET> a;
+  for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int t_end = min(ntiles, (ch + 1) * TILE_CHUNK);
+    for (int t = ch * TILE_CHUNK; t < t_end; t++) {
+      const BatchTile tile = tiles[t];
+      if (tile.slot != slot) {  // uniform across the block
+        slot = tile.slot;
+        const BatchCase& C = cases[slot];
+        const int remaining = C.remaining;
+        skip = !C.active || k >= remaining;
+        last = (remaining < K ? remaining : K) - 1;
+        const int parity = (C.counter + k) & 1;
+        a.src = C.buf[parity];
+        a.dst = C.buf[1 - parity];
+        a.stride = C.stride;
+        a.flags = C.flags;
+        a.nx = C.nx;
+        a.ny = C.ny;
+        a.nz = C.nz;
+        a.zone = static_cast<const R*>(C.zone);
+        a.glob = C.glob;
 #pragma unroll
-    for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
-    const int n = tile.start + threadIdx.x + blockDim.x * threadIdx.y;
-    const int sxy = a.nx * a.ny;
-    const bool act = n < sxy * a.nz;
-    const int z = n / sxy, r = n - z * sxy, y = r / a.nx, x = r - y * a.nx;
-    if (k == last) {
-      R g[M::NG];
+        for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
+      }
+      if (skip) continue;
+      const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
+      const bool act = x < a.nx && y < a.ny;
+      if (k == last) {
+        R g[M::NG];
 #pragma unroll
-      for (int i = 0; i < M::NG; i++) g[i] = 0;
-      if (act) node_update<M, R, St, true>(a, x, y, z, g);
-      reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
-      __syncthreads();  // shared scratch of reduce_globals reused by the next tile
-    } else if (act) {
-      R g[1];
-      node_update<M, R, St, false>(a, x, y, z, g);
+        for (int i = 0; i < M::NG; i++) g[i] = 0;
+        if (act) node_update<M, R, St, true>(a, x, y, z, g);
+        reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+        __syncthreads();  // shared scratch of reduce_globals reused by the next tile
+      } else if (act) {
+        R g[1];
+        node_update<M, R, St, false>(a, x, y, z, g);
+      }
     }
   }
 }

@@ -835,6 +835,96 @@ __device__ __forceinline__ void node_update(const Args<R, M::NSET>& a, int x, in
   for (int i = 0; i < M::Q; i++) St::template store<R>(dst + i * stride, f[i], R(M::w(i)));
 }
 
+// Two nodes per thread for 16-bit storage: (x, x+1) with x even, so every
+// population is one aligned 32-bit load and store and a warp moves 128 bytes
+// per request (with 2-byte values one node per thread moves only 64). The
+// pull shifts e_x = +1 / -1 take the neighbouring pair from the adjacent lane
+// by a shuffle; the lanes at the warp edges load their halo pair directly
+// (with the periodic wrap). Requires nx % 64 == 0 and whole warps on one row.
+template <class St>
+struct Pack16;
+template <bool SH>
+struct Pack16<StoreF16<SH>> {
+  __device__ __forceinline__ static float2 unpack(unsigned w) { return __half22float2(*reinterpret_cast<__half2*>(&w)); }
+  __device__ __forceinline__ static float lo(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+  __device__ __forceinline__ static float hi(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+  __device__ __forceinline__ static unsigned pack(float a, float b) {
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<unsigned*>(&h);
+  }
+};
+template <bool SH>
+struct Pack16<StoreBF16<SH>> {
+  __device__ __forceinline__ static float lo(unsigned w) { return __uint_as_float(w << 16); }
+  __device__ __forceinline__ static float hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+  __device__ __forceinline__ static float2 unpack(unsigned w) { return make_float2(lo(w), hi(w)); }
+  __device__ __forceinline__ static unsigned pack(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<unsigned*>(&h);
+  }
+};
+
+template <class M, class R, class St, bool G>
+__device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a, int x, int y, int z, int lane, R* g) {
+  using P = Pack16<St>;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int sxy = nx * ny;
+  const int node = x + nx * y + sxy * z;  // even
+  const int oy_lo = y == 0 ? nx * (ny - 1) : -nx, oy_hi = y + 1 == ny ? nx * (1 - ny) : nx;
+  const int oz_lo = z == 0 ? sxy * (nz - 1) : -sxy, oz_hi = z + 1 == nz ? sxy * (1 - nz) : sxy;
+  const int o_prev = x == 0 ? nx - 2 : -2;       // pair (x-2, x-1), wrapped
+  const int o_next = x + 2 == nx ? 2 - nx : 2;   // pair (x+2, x+3), wrapped
+  const unsigned short* __restrict__ src = static_cast<const unsigned short*>(a.src) + node;
+  unsigned short* __restrict__ dst = static_cast<unsigned short*>(a.dst) + node;
+  const size_t stride = a.stride;
+  const unsigned fl2 = __ldg(reinterpret_cast<const unsigned*>(a.flags + node));
+  R fa[M::Q], fb[M::Q];
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) {
+    const int o = (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0)) +
+                  (M::DIM == 2 ? 0 : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0)));
+    const unsigned short* p = src + i * stride + o;
+    const unsigned w = __ldg(reinterpret_cast<const unsigned*>(p));
+    const R sh = St::shifted ? R(M::w(i)) : R(0);
+    if (M::ex(i) == 0) {
+      const float2 v = P::unpack(w);
+      fa[i] = R(v.x) + sh;
+      fb[i] = R(v.y) + sh;
+    } else if (M::ex(i) > 0) {  // from x-1: (prev.hi, w.lo)
+      unsigned prev = __shfl_up_sync(0xffffffffu, w, 1);
+      if (lane == 0) prev = __ldg(reinterpret_cast<const unsigned*>(p + o_prev));
+      fa[i] = R(P::hi(prev)) + sh;
+      fb[i] = R(P::lo(w)) + sh;
+    } else {  // from x+1: (w.hi, next.lo)
+      unsigned next = __shfl_down_sync(0xffffffffu, w, 1);
+      if (lane == 31) next = __ldg(reinterpret_cast<const unsigned*>(p + o_next));
+      fa[i] = R(P::hi(w)) + sh;
+      fb[i] = R(P::lo(next)) + sh;
+    }
+  }
+  M::template run<R, G>(fa, (flag_t)(fl2 & 0xffffu), a, g);
+  M::template run<R, G>(fb, (flag_t)(fl2 >> 16), a, g);
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) {
+    const R sh = St::shifted ? R(M::w(i)) : R(0);
+    __stcs(reinterpret_cast<unsigned*>(dst + i * stride), P::pack((float)(fa[i] - sh), (float)(fb[i] - sh)));
+  }
+}
+
+// Block (32, by): each warp covers 64 consecutive x of one row.
+template <class M, class R, class St, bool G>
+__global__ void __launch_bounds__(256) k_iterate_pair(const Args<R, M::NSET> a) {
+  const int lane = threadIdx.x;
+  const int x = 2 * (blockIdx.x * 32 + lane);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  R g[G ? M::NG : 1];
+#pragma unroll
+  for (int i = 0; i < (G ? M::NG : 1); i++) g[i] = 0;
+  if (y < a.ny) node_update_pair<M, R, St, G>(a, x, y, z, lane, g);  // y is uniform per warp
+  if constexpr (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+}
+
 template <class M, class R, class St, bool G>
 __global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;

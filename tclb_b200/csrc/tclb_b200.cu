@@ -148,6 +148,7 @@ struct tclb_lattice {
   // settings travel as kernel parameters, so a settings change drops them.
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int use_graphs = 1;
+  int use_pairs = 1;  // 16-bit storage: two nodes per thread when nx % 64 == 0
 };
 
 struct Impl {
@@ -188,6 +189,14 @@ struct Launch {
     const void* src = L->buf[L->cur];
     void* dst = L->buf[1 - L->cur];
     auto a = make_args<M, R>(L, src, dst);
+    if constexpr (sizeof(typename St::T) == 2) {
+      if (L->use_pairs && L->nx % 64 == 0) {  // two nodes per thread, 32-bit accesses
+        const dim3 blk(32, 8), grd(L->nx / 64, (L->ny + 7) / 8, L->nz);
+        if (glob) k_iterate_pair<M, R, St, true><<<grd, blk, 0, s>>>(a);
+        else k_iterate_pair<M, R, St, false><<<grd, blk, 0, s>>>(a);
+        return;
+      }
+    }
     if (glob) k_iterate<M, R, St, true><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a);
     else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a);
   }
@@ -684,13 +693,14 @@ int tclb_get_iteration(tclb_h L, long long* iter) {
 
 double tclb_bytes_per_update(tclb_h L) { return L ? 2.0 * L->T->Q * L->elem + sizeof(flag_t) : 0.0; }
 
-int tclb_set_launch(tclb_h L, int bx, int by, int use_graphs) {
+int tclb_set_launch(tclb_h L, int bx, int by, int flags) {
   CHECK_H(L);
   if (bx < 32 || bx % 32 || by < 1 || bx * by > 256) return fail(TCLB_ERR_ARG, "bad block shape");
   drop_graphs(L);
   L->bx = bx;
   L->by = by;
-  L->use_graphs = use_graphs ? 1 : 0;
+  L->use_graphs = (flags & TCLB_LAUNCH_GRAPHS) ? 1 : 0;
+  L->use_pairs = (flags & TCLB_LAUNCH_PAIRS) ? 1 : 0;
   return TCLB_OK;
 }
 

@@ -287,3 +287,38 @@ def test_graph_replay_and_block_shape_do_not_change_results(shape):
         g.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.allclose(out[0][1], out[1][1], rtol=1e-12, atol=1e-18)
+
+
+@pytest.mark.parametrize("storage", ["fp16s", "bf16s"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_two_nodes_per_thread_path(model, storage):
+    """16-bit storage with nx % 64 == 0 updates two nodes per thread with
+    32-bit accesses and shuffles for the x shifts; it must agree with the
+    one-node path (a float rounding difference may flip a 16-bit rounding, so
+    the bar is 1e-3 relative L2 after a few iterations) and be as accurate
+    against the FP64 oracle."""
+    m = M.get(model)
+    shape = (1, 24, 128) if m.dim == 2 else (6, 10, 64)
+    fl = random_flags(model, shape, BOUNDARY_TYPES[model], zones=3, seed=7, p_type=0.2,
+                      extra_groups=EXTRA_GROUPS[model])
+    f0 = perturbed_equilibrium(model, shape, seed=8)
+    outs = []
+    for pairs in (False, True):
+        g = Lattice(model, shape[2], shape[1], shape[0], precision="fp32", storage=storage)
+        g.set_launch(32, 8, use_graphs=True, use_pairs=pairs)
+        g.set_flags(fl)
+        apply_params(g, PARAMS[model])
+        g.set_densities(f0)
+        g.Iterate(4, M.ITER_NORM | M.ITER_LASTGLOB)
+        outs.append((g.densities(), g.globals))
+        g.close()
+    o = oracle.OracleLattice(model, shape[2], shape[1], shape[0], precision="fp64")
+    o.set_flags(fl)
+    apply_params(o, PARAMS[model])
+    o.set_densities(f0)
+    o.iterate(4, M.ITER_NORM | M.ITER_LASTGLOB)
+    ref = o.densities()
+    assert np.isfinite(outs[1][0]).all()
+    assert rel_l2(outs[1][0], outs[0][0]) < 1e-3
+    e_single, e_pair = rel_l2(outs[0][0], ref), rel_l2(outs[1][0], ref)
+    assert e_pair < 1.5 * e_single + 1e-6, (e_single, e_pair)
