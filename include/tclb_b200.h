@@ -149,8 +149,10 @@ int tclb_sync(tclb_h h);
 
 /* Launch shape of the iteration kernel (bx multiple of 32, bx*by <= 256) and
    flags: TCLB_LAUNCH_GRAPHS replays runs of plain iterations from a captured
-   CUDA graph; TCLB_LAUNCH_PAIRS lets 16-bit storage with nx % 64 == 0 update
-   two nodes per thread with 32-bit accesses. Both are on by default. */
+   CUDA graph (on by default); TCLB_LAUNCH_PAIRS lets 16-bit storage with
+   nx % 64 == 0 update two nodes per thread with 32-bit accesses (off by
+   default: its register use halves the occupancy, which costs more than the
+   wider accesses gain on B200). */
 #define TCLB_LAUNCH_GRAPHS 1
 #define TCLB_LAUNCH_PAIRS 2
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);

@@ -148,7 +148,7 @@ struct tclb_lattice {
   // settings travel as kernel parameters, so a settings change drops them.
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int use_graphs = 1;
-  int use_pairs = 1;  // 16-bit storage: two nodes per thread when nx % 64 == 0
+  int use_pairs = 0;  // 16-bit storage: two nodes per thread when nx % 64 == 0 (opt-in)
 };
 
 struct Impl {
