@@ -85,6 +85,8 @@ int tclb_set_setting(tclb_h h, int setting, double value);
 int tclb_get_setting(tclb_h h, int setting, double* value);
 /* ZoneSettings::set (src/ZoneSettings.h:58-77); zone = -1 sets every zone. */
 int tclb_set_zone_setting(tclb_h h, int zone_setting, int zone, double value);
+/* ZoneSettings::get (src/ZoneSettings.h) for one zone. */
+int tclb_get_zone_setting(tclb_h h, int zone_setting, int zone, double* value);
 
 /* Lattice::Init (src/Lattice.cu.Rt:799-821): BaseInit stage (equilibrium
    from settings), resets the iteration counter and the Globals. */
@@ -156,6 +158,22 @@ int tclb_sync(tclb_h h);
 #define TCLB_LAUNCH_GRAPHS 1
 #define TCLB_LAUNCH_PAIRS 2
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);
+
+/* ---------------------------------------------------------------------------
+   XML case files (<CLBConfig>): the control flow of TCLB's main and handler
+   tree for the Run path (src/main.cpp:173-425, src/Handlers/acGeometry.cpp,
+   acModel.cpp, acParam.cpp, acInit.cpp, acSolve.cpp, cbLog.cpp, cbBIN.cpp,
+   cbFailcheck.cpp). Values may carry unit suffixes; <Units> gauges are not
+   supported (values are lattice units).
+   ------------------------------------------------------------------------- */
+const char* tclb_case_last_error(void);
+/* Node types of a case's <Geometry>, rasterised like src/Geometry.cpp.Rt with
+   nx padded to a multiple of 32 (src/Solver.cpp.Rt:273). dims gets nx, ny, nz;
+   pass flags = NULL to query the size first. */
+int tclb_case_geometry(const char* xml_text, int model, int dims[3], uint16_t* flags, size_t capacity);
+/* Run a case file for one model. Output files are named like
+   Solver::outIterFile (src/Solver.h.Rt:102-105): <out_dir><case>_<Log|BIN>_P00_<iteration>... */
+int tclb_case_run(const char* xml_path, int model, int precision, int storage, const char* out_dir, int verbose);
 
 /* ---------------------------------------------------------------------------
    Batches: many independent cases of one model advanced together by one

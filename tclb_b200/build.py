@@ -16,8 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtclb_b200.so")
-SOURCES = ["tclb_b200.cu", "batch.cu"]
-HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "tclb_models.h", "cumulant_gen.cuh"]
+SOURCES = ["tclb_b200.cu", "batch.cu", "case.cpp"]
+HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "tclb_models.h", "cumulant_gen.cuh", "xml.hpp"]
+RUNNER = os.path.join(HERE, "tclb_run")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -48,6 +49,12 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd, cwd=CSRC)
+    # the case-file runner executable, linked against the library
+    runner = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17", "-o", RUNNER, os.path.join(CSRC, "tclb_run.cpp"), "-L" + HERE,
+              "-ltclb_b200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+    if verbose:
+        print(" ".join(runner), flush=True)
+    subprocess.check_call(runner, cwd=CSRC)
     return LIB
 
 

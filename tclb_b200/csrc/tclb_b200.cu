@@ -92,16 +92,23 @@ const int d3q27c_nt_m[] = {3, 3, 4, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x78, 0x
 const char* const d3q27c_q[] = {"P", "U", "Solid"};
 const int d3q27c_qv[] = {0, 1, 0};
 
+const char* const d2q9_grp[] = {"BOUNDARY", "COLLISION", "OBJECTIVE"};
+const int d2q9_grp_m[] = {0xF, 0x10, 0x60};
+const char* const d3q19_grp[] = {"ADDITIONALS", "BOUNDARY", "COLLISION"};
+const int d3q19_grp_m[] = {0x3, 0x1C, 0x20};
+const char* const d3q27c_grp[] = {"ADDITIONALS", "BODY", "BOUNDARY", "COLLISION"};
+const int d3q27c_grp_m[] = {0x3, 0x4, 0x78, 0x80};
+
 const ModelTable TABLES[3] = {
     {"d2q9", 9, 2, d2q9::NSET, d2q9::NZS, d2q9::NG, d2q9::NSUM, d2q9::G_Objective, d2q9::IN_OBJ_OFFSET,
      d2q9::ZONE_SHIFT, d2q9_set, d2q9_set_def, d2q9_set_der, d2q9_zs, d2q9_zs_def, d2q9_gl, d2q9_nt, d2q9_nt_v,
-     d2q9_nt_m, 13, d2q9_q, d2q9_qv, 2},
+     d2q9_nt_m, 13, d2q9_q, d2q9_qv, 2, d2q9_grp, d2q9_grp_m, 3},
     {"d3q19", 19, 3, d3q19::NSET, d3q19::NZS, d3q19::NG, d3q19::NSUM, d3q19::G_Objective, d3q19::IN_OBJ_OFFSET,
      d3q19::ZONE_SHIFT, d3q19_set, d3q19_set_def, d3q19_set_der, d3q19_zs, d3q19_zs_def, d3q19_gl, d3q19_nt,
-     d3q19_nt_v, d3q19_nt_m, 10, d3q19_q, d3q19_qv, 2},
+     d3q19_nt_v, d3q19_nt_m, 10, d3q19_q, d3q19_qv, 2, d3q19_grp, d3q19_grp_m, 3},
     {"d3q27_cumulant", 27, 3, d3q27c::NSET, d3q27c::NZS, d3q27c::NG, d3q27c::NSUM, d3q27c::G_Objective,
      d3q27c::IN_OBJ_OFFSET, d3q27c::ZONE_SHIFT, d3q27c_set, d3q27c_set_def, d3q27c_set_der, d3q27c_zs, d3q27c_zs_def,
-     d3q27c_gl, d3q27c_nt, d3q27c_nt_v, d3q27c_nt_m, 16, d3q27c_q, d3q27c_qv, 3},
+     d3q27c_gl, d3q27c_nt, d3q27c_nt_v, d3q27c_nt_m, 16, d3q27c_q, d3q27c_qv, 3, d3q27c_grp, d3q27c_grp_m, 4},
 };
 
 // Derived-setting equations (each model's Dynamics.R AddSetting(..., X='expr'))
@@ -512,6 +519,14 @@ int tclb_set_zone_setting(tclb_h L, int s, int zone, double v) {
   else
     L->zone[(size_t)zone * nzs + s] = v;
   return upload_zone(L);
+}
+
+int tclb_get_zone_setting(tclb_h L, int s, int zone, double* v) {
+  CHECK_H(L);
+  if (s < 0 || s >= L->T->nzonesettings || zone < 0 || zone >= L->nzones || !v)
+    return fail(TCLB_ERR_ARG, "zone setting or zone out of range");
+  *v = L->zone[(size_t)zone * L->T->nzonesettings + s];
+  return TCLB_OK;
 }
 
 int tclb_init(tclb_h L) {

@@ -30,6 +30,9 @@ struct ModelTable {
   const char* const* quantity_names;
   const int* quantity_vector;
   int nquantities;
+  const char* const* group_names;  // node-type groups and their masks
+  const int* group_masks;
+  int ngroups;
 };
 
 // ---------------------------------------------------------------- d2q9

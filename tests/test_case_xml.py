@@ -1,0 +1,141 @@
+"""XML case front-end (tclb_case_geometry / tclb_case_run): the native C++
+rasteriser against the Python one and hand-computed shapes (CPU), and a case
+file run end to end against the API (GPU)."""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from tclb_b200 import cases
+from tclb_b200 import models as M
+from tclb_b200.lattice import load_library
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def case_geometry(xml: str, model: str) -> np.ndarray:
+    lib = load_library()
+    lib.tclb_case_geometry.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_uint16), ctypes.c_size_t]
+    lib.tclb_case_last_error.restype = ctypes.c_char_p
+    dims = (ctypes.c_int * 3)()
+    mid = M.get(model).mid
+    assert lib.tclb_case_geometry(xml.encode(), mid, dims, None, 0) == 0, lib.tclb_case_last_error()
+    nx, ny, nz = dims
+    out = np.zeros((nz, ny, nx), np.uint16)
+    rc = lib.tclb_case_geometry(xml.encode(), mid, dims, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), out.size)
+    assert rc == 0, lib.tclb_case_last_error()
+    return out
+
+
+def test_channel_disc_matches_python_rasteriser():
+    xml = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    fl = case_geometry(xml, "d2q9")
+    assert fl.shape == (1, 64, 256)  # nx padded 250 -> 256 (src/Solver.cpp.Rt:273)
+    ref = cases.channel_disc_d2q9(256, 64, r=8, cx=64, cy=32)
+    assert np.array_equal(fl, ref)
+
+
+def test_tunnel_text_and_modes_d3q19(tmp_path):
+    m = M.get("d3q19")
+    rng = np.random.default_rng(0)
+    pts = (rng.random((4, 8, 6)) < 0.3).astype(int)  # x outer, y, z inner
+    f = tmp_path / "solid.txt"
+    f.write_text(" ".join(str(v) for v in pts.ravel()))
+    xml = f"""<CLBConfig><Geometry nx="32" ny="12" nz="10">
+      <MRT><Box/></MRT>
+      <Wall mask="ALL"><Tunnel/></Wall>
+      <Solid mode="fill"><Text file="{f}" dx="4" nx="4" dy="2" ny="8" dz="2" nz="6"/></Solid>
+      <WVelocity name="in" mode="change"><Box nx="1"/></WVelocity>
+    </Geometry></CLBConfig>"""
+    fl = case_geometry(xml, "d3q19")
+    g = cases.Geometry("d3q19", 32, 12, 10)
+    g.set_flag("MRT").box()
+    g.set_flag("Wall", mask="ALL").tunnel()
+    g.set_flag("Solid", mode="fill")
+    sel = np.zeros((10, 12, 32), bool)
+    for x in range(4):
+        for y in range(8):
+            for z in range(6):
+                if pts[x, y, z]:
+                    sel[2 + z, 2 + y, 4 + x] = True
+    cur = g.geom[sel]
+    keep = (cur & g.mask) != 0
+    cur[~keep] = (cur[~keep] & (~g.mask & 0xFFFF)) | g.fg
+    g.geom[sel] = cur
+    g.set_flag("WVelocity", zone="in", mode="change").box(nx=1)
+    assert np.array_equal(fl, g.geom)
+    assert (fl[:, :, 0] >> m.zone_shift).max() == 1
+
+
+def test_wedge_and_units():
+    xml = """<CLBConfig><Geometry nx="32" ny="8">
+      <Wall><Wedge dx="2" nx="5" dy="1" ny="5" direction="LowerRight"/></Wall>
+      <Solid><Box dx="20mm" nx="1m" dy="0" ny="1"/></Solid>
+    </Geometry></CLBConfig>"""
+    fl = case_geometry(xml, "d2q9")
+    wall = M.get("d2q9").flag("Wall")
+    got = {(x, y) for y in range(8) for x in range(32) if fl[0, y, x] == wall}
+    # inWedge LowerRight: (1-x) - (1-y) < 1e-10 on the 5x5 box at (2,1)
+    want = {(2 + i, 1 + j) for i in range(5) for j in range(5) if (1 - i / 4) - (1 - j / 4) < 1e-10}
+    assert got == want
+    assert fl[0, 0, 0] == M.get("d2q9").flag("Solid")  # 20mm -> 0.02 -> column 0, 1m -> nx=1
+
+
+def test_bad_case_is_an_error_not_an_exit():
+    lib = load_library()
+    lib.tclb_case_last_error.restype = ctypes.c_char_p
+    dims = (ctypes.c_int * 3)()
+    rc = lib.tclb_case_geometry(b"<CLBConfig><Geometry nx='8' ny='8'><Wal><Box/></Wal></Geometry></CLBConfig>",
+                                0, dims, None, 0)
+    assert rc == 0  # size query does not rasterise
+    out = np.zeros(8 * 32, np.uint16)
+    rc = lib.tclb_case_geometry(b"<CLBConfig><Geometry nx='8' ny='8'><Wal><Box/></Wal></Geometry></CLBConfig>",
+                                0, dims, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), out.size)
+    assert rc != 0 and b"Wal" in lib.tclb_case_last_error()
+    rc = lib.tclb_case_geometry(b"<CLBConfig><Geometry nx='8'>", 0, dims, None, 0)
+    assert rc != 0 and b"XML" in lib.tclb_case_last_error()
+
+
+@pytest.mark.gpu
+def test_case_file_run_matches_api(tmp_path):
+    """tclb_run on the channel case: the Log CSV rows and the final BIN files
+    equal what the Python API produces for the same flags and settings."""
+    import subprocess
+
+    from tclb_b200.lattice import Lattice
+
+    xml = os.path.join(HERE, "cases", "channel_disc.xml")
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    out = str(tmp_path) + "/"
+    r = subprocess.run([runner, "d2q9", xml, "--output", out, "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    logs = glob.glob(out + "channel_disc_Log_P00_00000000.csv")
+    assert logs, os.listdir(out)
+    rows = open(logs[0]).read().strip().splitlines()
+    hdr = [h.strip('"') for h in rows[0].split(",")]
+    data = np.array([[float(v) for v in r.split(",")] for r in rows[1:]])
+    assert list(data[:, 0]) == [50, 100, 150, 200]
+    # the same through the API
+    m = M.get("d2q9")
+    lat = Lattice("d2q9", 256, 64)
+    lat.set_flags(cases.channel_disc_d2q9(256, 64, r=8, cx=64, cy=32))
+    lat.set_zone_setting("VelocityX", 0.01)
+    lat.SetSetting("Viscosity", 0.02)
+    lat.SetSetting("S3", -0.7857142857142858)
+    lat.SetSetting("S4", -0.7857142857142858)
+    lat.Init()
+    for k in range(4):
+        lat.Iterate(50, M.ITER_NORM | M.ITER_LASTGLOB)
+        g = lat.globals
+        for gi, (gname, _op) in enumerate(m.globals):
+            assert data[k, hdr.index(gname)] == pytest.approx(g[gi], rel=1e-6, abs=1e-12)
+    assert data[-1, hdr.index("S2")] == pytest.approx(1 - 1 / (3 * 0.02 + 0.5))
+    assert data[-1, hdr.index("VelocityX-Inlet")] == pytest.approx(0.01)
+    u = np.fromfile(out + "channel_disc_BIN_P00_00000200.U.bin", dtype=np.float32).reshape(1, 64, 256, 3)
+    assert np.array_equal(u, lat.GetQuantity("U"))
+    rho = np.fromfile(out + "channel_disc_BIN_P00_00000200.Rho.bin", dtype=np.float32)
+    assert rho.size == 64 * 256
+    lat.close()
