@@ -141,6 +141,15 @@ size_t tclb_snapshot_bytes(tclb_h h);
 int tclb_save(tclb_h h, void* host, size_t bytes, void* stream);
 int tclb_load(tclb_h h, const void* host, size_t bytes, void* stream);
 
+/* TCLB's .pri checkpoint of the current snapshot (Lattice::save / load,
+   src/Lattice.cu.Rt:642-769): the snapshot's non-empty margin blocks in block
+   order, each an x-fastest box of storage_t values per density (the interior
+   block plus the ghost copies one rank keeps of the opposite faces). Loading
+   reads the interior block. */
+size_t tclb_pri_bytes(tclb_h h);
+int tclb_save_pri(tclb_h h, void* host, size_t bytes);
+int tclb_load_pri(tclb_h h, const void* host, size_t bytes);
+
 /* Iterations done since Init, and the bytes one iteration moves
    (2*Q*sizeof(storage_t) + sizeof(flag_t) per node). */
 int tclb_get_iteration(tclb_h h, long long* iter);

@@ -319,6 +319,8 @@ int pad_nx(int nx, int xsdim = 32) { return nx + xsdim - 1 - ((nx - 1) % xsdim);
 
 // ------------------------------------------------------------------ runner
 struct Runner;
+std::string read_file(const std::string& path);
+void write_xml(std::ostream& o, const XmlNode* n, int depth);
 
 struct Callback {
   std::string kind;  // Log, BIN, Failcheck
@@ -350,6 +352,8 @@ struct Runner {
   int iter_type = TCLB_ITER_NORM;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   bool verbose = true;
+  std::string config_text;
+  std::vector<std::string> checkpoints;
 
   ~Runner() {
     if (lat) tclb_destroy(lat);
@@ -496,6 +500,66 @@ struct Runner {
     return false;
   }
 
+  // <LoadBinary file=> (src/Handlers/acLoadBinary.cpp): Lattice::loadSolution
+  // reads <file>_0.pri (rank 0) into the current snapshot.
+  void load_binary(const XmlNode* n) {
+    need_lattice();
+    const std::string* f = n->attr("file");
+    if (!f) f = n->attr("filename");
+    if (!f) throw CaseError("<LoadBinary> needs a file attribute");
+    if (n->attr("comp")) throw CaseError("<LoadBinary comp=> (single fields) is not supported");
+    const std::string fn = *f + "_0.pri";
+    const std::string data = read_file(fn);
+    if (data.size() != tclb_pri_bytes(lat)) throw CaseError(fn + " does not match this lattice");
+    ck(tclb_load_pri(lat, data.data(), data.size()), "load .pri");
+  }
+  // <SaveCheckpoint> (src/Handlers/cbSaveCheckpoint.cpp:37-104): .pri plus a
+  // restart case that loads it before <Solve>; keep = number retained.
+  void save_checkpoint(const Callback& c) {
+    char it[32];
+    std::snprintf(it, sizeof(it), "_%08lld", iter);
+    const std::string base = outpath + "_checkpoint" + it;
+    std::vector<char> buf(tclb_pri_bytes(lat));
+    ck(tclb_save_pri(lat, buf.data(), buf.size()), "save .pri");
+    const std::string pri = base + "_0.pri";
+    FILE* o = std::fopen(pri.c_str(), "wb");
+    if (!o) throw CaseError("cannot write " + pri);
+    std::fwrite(buf.data(), 1, buf.size(), o);
+    std::fclose(o);
+    // restart file: the case with <LoadBinary file=base> before the first <Solve>
+    auto doc = XmlParser(config_text).parse();
+    XmlNode* cfg = nullptr;
+    for (auto& ch : doc->children)
+      if (ch->name == "CLBConfig") cfg = ch.get();
+    if (cfg) {
+      auto lb = std::make_unique<XmlNode>();
+      lb->name = "LoadBinary";
+      lb->attrs.emplace_back("file", base);
+      lb->parent = cfg;
+      size_t pos = cfg->children.size();
+      for (size_t i = 0; i < cfg->children.size(); i++)
+        if (cfg->children[i]->name == "LoadBinary") {
+          cfg->children.erase(cfg->children.begin() + i);
+          break;
+        }
+      for (size_t i = 0; i < cfg->children.size(); i++)
+        if (cfg->children[i]->name == "Solve") {
+          pos = i;
+          break;
+        }
+      cfg->children.insert(cfg->children.begin() + pos, std::move(lb));
+      std::ofstream rf(outpath + "_restart" + it + ".xml");
+      rf << "<?xml version=\"1.0\"?>\n";
+      write_xml(rf, cfg, 0);
+    }
+    const int keep = c.node->attr("keep") ? parse_int(*c.node->attr("keep")) : 1;
+    checkpoints.push_back(base);
+    while (keep > 0 && (int)checkpoints.size() > keep) {
+      std::remove((checkpoints.front() + "_0.pri").c_str());
+      checkpoints.erase(checkpoints.begin());
+    }
+  }
+
   // Handler of a callback element; returns true when it registered (has Iterations)
   bool callback(const XmlNode* n) {
     need_lattice();
@@ -520,6 +584,7 @@ struct Runner {
   bool do_callback(const Callback& c) {
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
+    else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
     else if (c.kind == "Failcheck") {
       if (failcheck()) {
         std::printf("[tclb_run] Failcheck: non-finite values at iteration %lld, stopping\n", iter);
@@ -574,7 +639,9 @@ struct Runner {
       } else if (n->name == "Param") param(n);
       else if (n->name == "Init") init();
       else if (n->name == "Solve") solve(n);
-      else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck") callback(n);
+      else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint")
+        callback(n);
+      else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {
         if (!n->children.empty()) throw CaseError("<Units> gauges are not supported: give values in lattice units");
       } else if (n->name == "VTK" || n->name == "TXT" || n->name == "Stop" || n->name == "Average") {
@@ -585,6 +652,31 @@ struct Runner {
     }
   }
 };
+
+std::string xml_escape(const std::string& v) {
+  std::string o;
+  for (char c : v) {
+    if (c == '&') o += "&amp;";
+    else if (c == '<') o += "&lt;";
+    else if (c == '>') o += "&gt;";
+    else if (c == '"') o += "&quot;";
+    else o += c;
+  }
+  return o;
+}
+
+void write_xml(std::ostream& o, const XmlNode* n, int depth) {
+  const std::string ind(depth, '\t');
+  o << ind << "<" << n->name;
+  for (const auto& a : n->attrs) o << " " << a.first << "=\"" << xml_escape(a.second) << "\"";
+  if (n->children.empty()) {
+    o << "/>\n";
+    return;
+  }
+  o << ">\n";
+  for (const auto& c : n->children) write_xml(o, c.get(), depth + 1);
+  o << ind << "</" << n->name << ">\n";
+}
 
 std::string read_file(const std::string& path) {
   std::ifstream in(path, std::ios::binary);
@@ -648,6 +740,7 @@ int tclb_case_run(const char* xml_path, int model, int precision, int storage, c
     R.T = model_table(model);
     if (!R.T) throw CaseError("unknown model");
     const std::string text = read_file(xml_path);
+    R.config_text = text;
     auto doc = XmlParser(text).parse();
     const XmlNode* cfg = doc->child("CLBConfig");
     if (!cfg) throw CaseError("no <CLBConfig> element");

@@ -700,6 +700,111 @@ int tclb_load(tclb_h L, const void* host, size_t bytes, void* stream) {
   return TCLB_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// TCLB's .pri snapshot (Lattice::save / load, src/Lattice.cu.Rt:642-769): the
+// non-empty margin blocks of a snapshot, block k = 1..27 with offsets
+// (dx,dy,dz) = ((k-1)%3-1, ((k-1)/3)%3-1, (k-1)/9-1), concatenated. Block
+// (0,0,0) is the interior; a margin block holds, for every density that is
+// pulled across that face/edge/corner, the values its ghost layer carries --
+// on one rank the wrapped values of the opposite side -- as an x-fastest box
+// (src/conf.R:771-1023 with the default GPU layout). Fields are in density
+// order, values in storage_t.
+// ---------------------------------------------------------------------------
+namespace {
+struct PriBlock {
+  int d[3];
+  std::vector<int> fields;
+  int n[3];
+};
+
+template <class M>
+std::vector<PriBlock> pri_blocks_m(int nx, int ny, int nz) {
+  std::vector<PriBlock> out;
+  const int dims[3] = {nx, ny, nz};
+  for (int k = 0; k < 27; k++) {
+    PriBlock b;
+    b.d[0] = k % 3 - 1;
+    b.d[1] = (k / 3) % 3 - 1;
+    b.d[2] = k / 9 - 1;
+    for (int i = 0; i < M::Q; i++) {
+      const int e[3] = {M::ex(i), M::ey(i), M::ez(i)};
+      bool in = true;
+      for (int a = 0; a < 3; a++) in = in && (b.d[a] == 0 || e[a] == -b.d[a]);  // pulled across this side
+      if (in) b.fields.push_back(i);
+    }
+    for (int a = 0; a < 3; a++) b.n[a] = b.d[a] == 0 ? dims[a] : 1;
+    if (!b.fields.empty()) out.push_back(b);
+  }
+  return out;
+}
+
+std::vector<PriBlock> pri_blocks(const tclb_lattice* L) {
+  switch (L->model) {
+    case MODEL_D2Q9: return pri_blocks_m<D2Q9>(L->nx, L->ny, L->nz);
+    case MODEL_D3Q19: return pri_blocks_m<D3Q19>(L->nx, L->ny, L->nz);
+    default: return pri_blocks_m<D3Q27C>(L->nx, L->ny, L->nz);
+  }
+}
+
+size_t pri_size(const tclb_lattice* L) {
+  size_t s = 0;
+  for (const auto& b : pri_blocks(L)) s += b.fields.size() * (size_t)b.n[0] * b.n[1] * b.n[2] * L->elem;
+  return s;
+}
+}  // namespace
+
+extern "C" {
+
+size_t tclb_pri_bytes(tclb_h L) { return L ? pri_size(L) : 0; }
+
+int tclb_save_pri(tclb_h L, void* host, size_t bytes) {
+  CHECK_H(L);
+  if (!host || bytes != pri_size(L)) return fail(TCLB_ERR_ARG, ".pri buffer size mismatch");
+  std::vector<char> raw(L->stride * L->T->Q * L->elem);
+  TCLB_CK(cudaMemcpyAsync(raw.data(), L->buf[L->cur], raw.size(), cudaMemcpyDeviceToHost, L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  char* o = static_cast<char*>(host);
+  const size_t e = L->elem;
+  for (const auto& b : pri_blocks(L))
+    for (int i : b.fields)
+      for (int z = 0; z < b.n[2]; z++)
+        for (int y = 0; y < b.n[1]; y++)
+          for (int x = 0; x < b.n[0]; x++) {
+            // ghost at -1 carries the value of the last layer, ghost at +n the first
+            const int sx = b.d[0] < 0 ? L->nx - 1 : (b.d[0] > 0 ? 0 : x);
+            const int sy = b.d[1] < 0 ? L->ny - 1 : (b.d[1] > 0 ? 0 : y);
+            const int sz = b.d[2] < 0 ? L->nz - 1 : (b.d[2] > 0 ? 0 : z);
+            const size_t n = (size_t)sx + (size_t)L->nx * ((size_t)sy + (size_t)L->ny * sz);
+            std::memcpy(o, raw.data() + ((size_t)i * L->stride + n) * e, e);
+            o += e;
+          }
+  return TCLB_OK;
+}
+
+int tclb_load_pri(tclb_h L, const void* host, size_t bytes) {
+  CHECK_H(L);
+  if (!host || bytes != pri_size(L)) return fail(TCLB_ERR_ARG, ".pri buffer size mismatch");
+  const char* in = static_cast<const char*>(host);
+  const size_t e = L->elem;
+  std::vector<char> raw(L->stride * L->T->Q * L->elem, 0);
+  for (const auto& b : pri_blocks(L)) {
+    const size_t box = (size_t)b.n[0] * b.n[1] * b.n[2];
+    if (b.d[0] == 0 && b.d[1] == 0 && b.d[2] == 0) {  // the interior carries the state
+      for (int i : b.fields) {
+        std::memcpy(raw.data() + (size_t)i * L->stride * e, in, box * e);
+        in += box * e;
+      }
+    } else {
+      in += b.fields.size() * box * e;
+    }
+  }
+  TCLB_CK(cudaMemcpyAsync(L->buf[L->cur], raw.data(), raw.size(), cudaMemcpyHostToDevice, L->stream));
+  TCLB_CK(cudaStreamSynchronize(L->stream));
+  return TCLB_OK;
+}
+
 int tclb_get_iteration(tclb_h L, long long* iter) {
   CHECK_H(L);
   if (iter) *iter = L->iter;

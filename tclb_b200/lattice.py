@@ -72,6 +72,10 @@ def load_library(path: Optional[str] = None):
     L.tclb_bytes_per_update.restype = d
     L.tclb_sync.argtypes = [h]
     L.tclb_set_launch.argtypes = [h, i, i, i]
+    L.tclb_pri_bytes.argtypes = [h]
+    L.tclb_pri_bytes.restype = sz
+    L.tclb_save_pri.argtypes = [h, vp, sz]
+    L.tclb_load_pri.argtypes = [h, vp, sz]
     _lib = L
     return L
 
@@ -227,6 +231,16 @@ class Lattice:
         n = self.snapshot_bytes()
         ptr = buf.ctypes.data if hasattr(buf, "ctypes") else buf
         _check(self.lib.tclb_load(self._h, ctypes.c_void_p(ptr), n, ctypes.c_void_p(stream or None)))
+
+    def save_pri(self) -> np.ndarray:
+        """TCLB's .pri layout of the current snapshot (margin blocks concatenated)."""
+        buf = np.empty(int(self.lib.tclb_pri_bytes(self._h)), np.uint8)
+        _check(self.lib.tclb_save_pri(self._h, ctypes.c_void_p(buf.ctypes.data), buf.size))
+        return buf
+
+    def load_pri(self, buf: np.ndarray):
+        b = np.ascontiguousarray(buf, np.uint8)
+        _check(self.lib.tclb_load_pri(self._h, ctypes.c_void_p(b.ctypes.data), b.size))
 
     @property
     def iteration(self) -> int:
