@@ -116,6 +116,14 @@ int tclb_clear_globals(tclb_h h);
    TCLB_FP32, double for TCLB_FP64); vector quantities are 3 values per node. */
 int tclb_get_quantity(tclb_h h, int q, const int region[6], void* out, double scale, void* stream);
 
+/* Lattice::Color (src/Lattice.cu.Rt:791-793 -> LatticeContainer::Color,
+   src/LatticeContainer.inc.cpp.Rt:350-423), headless: nx*ny RGBA bytes (uchar4,
+   x fastest) of plane z (z < 0: nz/2, the plane TCLB draws) from the model's
+   Color() through TCLB's colour map. `rgba` is device memory, written
+   asynchronously on `stream`, or host memory when on_host != 0 (the call then
+   returns after the copy). */
+int tclb_color(tclb_h h, void* rgba, int z, int on_host, void* stream);
+
 /* Same result as tclb_get_quantity, for callers that must not allocate device
    memory: an application whose GPU memory is all owned by its own pool or
    admission budget, or a latency-critical loop where cudaMalloc/cudaFree would
@@ -143,9 +151,11 @@ int tclb_load(tclb_h h, const void* host, size_t bytes, void* stream);
 
 /* TCLB's .pri checkpoint of the current snapshot (Lattice::save / load,
    src/Lattice.cu.Rt:642-769): the snapshot's non-empty margin blocks in block
-   order, each an x-fastest box of storage_t values per density (the interior
-   block plus the ghost copies one rank keeps of the opposite faces). Loading
-   reads the interior block. */
+   order, each an x-fastest box of storage_t values per density, byte for byte
+   what a single-rank TCLB run of the same model and storage writes: an edge
+   node's outgoing density sits in the margin block it is pulled from (and, for
+   d3q27_cumulant only, in place as well); slots TCLB never writes are zero.
+   Loading takes each node's value from the block it is pulled from. */
 size_t tclb_pri_bytes(tclb_h h);
 int tclb_save_pri(tclb_h h, void* host, size_t bytes);
 int tclb_load_pri(tclb_h h, const void* host, size_t bytes);

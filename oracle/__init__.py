@@ -52,6 +52,8 @@ def lib():
         L.orc_d2q9_basis.argtypes = [dp, ctypes.POINTER(ctypes.c_int)]
         L.orc_node_type_value.argtypes = [i, ctypes.c_char_p]
         L.orc_node_update.argtypes = [vp, dp, ctypes.c_uint16, dp]
+        L.orc_color.argtypes = [vp, i, vp]
+        L.orc_color_map.argtypes = [vp, vp, i, vp]
         _lib = L
     return _lib
 
@@ -138,11 +140,27 @@ class OracleLattice:
         assert a.size == self.model.Q * self.N
         lib().orc_set_densities(self._h, _dp(a))
 
+    def color(self, z: int = -1) -> np.ndarray:
+        """Headless ColorKernel of plane z (default nz/2): (ny, nx, 4) RGBA."""
+        out = np.zeros((self.ny, self.nx, 4), np.uint8)
+        lib().orc_color(self._h, self.nz // 2 if z < 0 else z, out.ctypes.data)
+        return out
+
     def node_update(self, fin, flag: int) -> np.ndarray:
         a = np.ascontiguousarray(fin, dtype=np.float64)
         out = np.zeros(self.model.Q)
         lib().orc_node_update(self._h, _dp(a), flag, _dp(out))
         return out
+
+
+def color_map(l, w) -> np.ndarray:
+    """ColorKernel's colour map of float l = |U| and weight w: (n, 4) RGBA."""
+    la = np.asarray(l, np.float32)
+    lv = np.ascontiguousarray(la).ravel()
+    wv = np.ascontiguousarray(np.broadcast_to(np.asarray(w, np.float32), la.shape)).ravel()
+    out = np.zeros((lv.size, 4), np.uint8)
+    lib().orc_color_map(lv.ctypes.data, wv.ctypes.data, lv.size, out.ctypes.data)
+    return out
 
 
 def feq(model, rho: float, J) -> np.ndarray:

@@ -1183,6 +1183,53 @@ struct Lattice {
   }
 };
 
+// ColorKernel's colour map (src/LatticeContainer.inc.cpp.Rt:378-401): the
+// fraction branches in float, truncated to int; w scales the colour towards
+// green; a non-finite l is magenta. Built without FP contraction.
+void color_map(float l, float w, uint8_t* o) {
+  int r = 0, g = 0, b = 0;
+  if (std::isfinite(l)) {
+    l = l * 111;
+    if (l < -111) { r = 255; g = 255; b = 255; }
+    if ((l >= -111) && (l < -11)) { r = 255 * (-l - 11) / 100; g = 255; b = 255; }
+    if ((l >= -11) && (l < -1)) { r = 0; g = (255 * (-l - 1)) / 10; b = 255; }
+    if ((l >= -1) && (l < 0)) { r = 0; g = 0; b = 255 * (-l); }
+    if ((l >= 0) && (l < 1)) { r = 255 * l; g = 0; b = 0; }
+    if ((l >= 1) && (l < 11)) { r = 255; g = 255 * (l - 1) / 10; b = 0; }
+    if ((l >= 11) && (l < 111)) { r = 255; g = 255; b = 255 * (l - 11) / 100; }
+    if (l >= 111) { r = 255; g = 255; b = 255; }
+    r = r * w;
+    g = g * w + (1 - w) * 255;
+    b = b * w;
+  } else {
+    r = 255; b = 255; g = 0;
+  }
+  o[0] = (uint8_t)r; o[1] = (uint8_t)g; o[2] = (uint8_t)b; o[3] = 255;
+}
+
+// Color() of each model: l = |U| from getU, w = 0 on the drawn-blank nodes
+// (d2q9/Dynamics.c.Rt:61-71 and d3q27_cumulant/Dynamics.c.Rt:101-111: the
+// flag equal to Solid; d3q19/Dynamics.c.Rt:42-52: BOUNDARY group == Wall)
+template <class R>
+void color_plane(const Lattice<R>& L, int z, uint8_t* out) {
+  std::vector<double> u((size_t)3 * L.nx * L.ny * L.nz);
+  L.quantity(1, u.data());
+  for (int y = 0; y < L.ny; y++)
+    for (int x = 0; x < L.nx; x++) {
+      const size_t n = L.nidx(x, y, z);
+      const R ux = (R)u[3 * n], uy = (R)u[3 * n + 1], uz = (R)u[3 * n + 2];
+      R s = ux * ux + uy * uy;
+      if (L.model != M_D2Q9) s = s + uz * uz;
+      const float l = (float)std::sqrt(s);
+      const flag_t fl = L.flags[n];
+      float w = 1;
+      if (L.model == M_D2Q9) w = fl == 9 ? 0.f : 1.f;
+      else if (L.model == M_D3Q19) w = (fl & 0x1C) == 0x0C ? 0.f : 1.f;
+      else w = fl == 0x48 ? 0.f : 1.f;
+      color_map(l, w, out + 4 * ((size_t)x + (size_t)L.nx * y));
+    }
+}
+
 struct Handle {
   int precision;  // 0 fp32, 1 fp64
   Lattice<float>* lf = nullptr;
@@ -1313,6 +1360,17 @@ int orc_set_densities(void* p, const double* in) {
 
 // Equilibrium distribution from the oracle's own construction (used by tests
 // to cross-check the product's closed forms).
+int orc_color(void* p, int z, uint8_t* out) {
+  Handle* h = (Handle*)p;
+  if (h->precision) color_plane(*h->ld, z, out); else color_plane(*h->lf, z, out);
+  return 0;
+}
+
+int orc_color_map(const float* l, const float* w, int n, uint8_t* out) {
+  for (int i = 0; i < n; i++) color_map(l[i], w[i], out + 4 * (size_t)i);
+  return 0;
+}
+
 int orc_feq(int model, double rho, const double* J, double* out) {
   Ops<double> o;
   o.build(model);

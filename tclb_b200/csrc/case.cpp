@@ -353,7 +353,7 @@ struct Runner {
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   bool verbose = true;
   std::string config_text;
-  std::vector<std::string> checkpoints;
+  std::vector<std::string> checkpoints, restarts;
 
   ~Runner() {
     if (lat) tclb_destroy(lat);
@@ -526,37 +526,63 @@ struct Runner {
     if (!o) throw CaseError("cannot write " + pri);
     std::fwrite(buf.data(), 1, buf.size(), o);
     std::fclose(o);
-    // restart file: the case with <LoadBinary file=base> before the first <Solve>
+    // restart file (writeRestartFile, cbSaveCheckpoint.cpp:80-101): the case
+    // with its <LoadBinary> pointed at this checkpoint, or a new one inserted
+    // before the first <Solve>
+    const std::string restart = outpath + "_restart" + it + ".xml";
     auto doc = XmlParser(config_text).parse();
     XmlNode* cfg = nullptr;
     for (auto& ch : doc->children)
       if (ch->name == "CLBConfig") cfg = ch.get();
     if (cfg) {
-      auto lb = std::make_unique<XmlNode>();
-      lb->name = "LoadBinary";
-      lb->attrs.emplace_back("file", base);
-      lb->parent = cfg;
-      size_t pos = cfg->children.size();
-      for (size_t i = 0; i < cfg->children.size(); i++)
-        if (cfg->children[i]->name == "LoadBinary") {
-          cfg->children.erase(cfg->children.begin() + i);
+      XmlNode* lb = nullptr;
+      for (auto& ch : cfg->children)
+        if (ch->name == "LoadBinary") {
+          lb = ch.get();
           break;
         }
-      for (size_t i = 0; i < cfg->children.size(); i++)
-        if (cfg->children[i]->name == "Solve") {
-          pos = i;
-          break;
-        }
-      cfg->children.insert(cfg->children.begin() + pos, std::move(lb));
-      std::ofstream rf(outpath + "_restart" + it + ".xml");
+      if (lb) {
+        for (size_t i = 0; i < lb->attrs.size(); i++)
+          if (lb->attrs[i].first == "file") {
+            lb->attrs.erase(lb->attrs.begin() + i);
+            break;
+          }
+        lb->attrs.emplace_back("file", base);
+      } else {
+        for (size_t i = 0; i < cfg->children.size(); i++)
+          if (cfg->children[i]->name == "Solve") {
+            auto n = std::make_unique<XmlNode>();
+            n->name = "LoadBinary";
+            n->attrs.emplace_back("file", base);
+            n->parent = cfg;
+            cfg->children.insert(cfg->children.begin() + i, std::move(n));
+            break;
+          }
+      }
+      std::ofstream rf(restart);
       rf << "<?xml version=\"1.0\"?>\n";
       write_xml(rf, cfg, 0);
     }
-    const int keep = c.node->attr("keep") ? parse_int(*c.node->attr("keep")) : 1;
+    // keep: "all" -> every checkpoint; n >= 0 -> the newest n (default 1)
+    int keep = 1;
+    if (const std::string* k = c.node->attr("keep")) {
+      if (*k == "all") keep = 0;
+      else {
+        keep = parse_int(*k);
+        if (keep < 0) {
+          std::fprintf(stderr, "[tclb_run] SaveCheckpoint keep < 0: keeping 1\n");
+          keep = 1;
+        }
+      }
+    }
+    if (keep == 0) return;
     checkpoints.push_back(base);
-    while (keep > 0 && (int)checkpoints.size() > keep) {
+    restarts.push_back(restart);
+    while ((int)checkpoints.size() > keep) {
       std::remove((checkpoints.front() + "_0.pri").c_str());
+      std::remove(restarts.front().c_str());
       checkpoints.erase(checkpoints.begin());
+      restarts.erase(restarts.begin());
     }
   }
 

@@ -263,6 +263,8 @@ struct D2Q9 {
     out[1] = jy / rho + a.s[d2q9::S_GravitationY] * R(0.5);
     out[2] = 0;
   }
+  // Color() (:61-71): |U| shaded, the whole flag equal to Solid drawn blank
+  __device__ __forceinline__ static float color_weight(flag_t fl) { return fl == d2q9::Solid ? 0.f : 1.f; }
 };
 
 // ---------------------------------------------------------------------------
@@ -518,6 +520,10 @@ struct D3Q19 {
     if ((fl & d3q19::BOUNDARY) == d3q19::Wall) { out[0] = out[1] = out[2] = 0; return; }
     out[0] = jx / rho; out[1] = jy / rho; out[2] = jz / rho;
   }
+  // Color() (:42-52): walls drawn blank
+  __device__ __forceinline__ static float color_weight(flag_t fl) {
+    return (fl & d3q19::BOUNDARY) == d3q19::Wall ? 0.f : 1.f;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -764,6 +770,8 @@ struct D3Q27C {
     out[1] = (jy + a.s[d3q27c::S_ForceY] / R(2)) / rho;
     out[2] = (jz + a.s[d3q27c::S_ForceZ] / R(2)) / rho;
   }
+  // Color() (:101-111): the whole flag equal to Solid drawn blank
+  __device__ __forceinline__ static float color_weight(flag_t fl) { return fl == d3q27c::Solid ? 0.f : 1.f; }
 };
 
 // ---------------------------------------------------------------------------
@@ -1003,6 +1011,72 @@ __global__ void k_quantity(const Args<R, M::NSET> a, int q, int vec, int rx, int
   } else {
     out[o] = v[0] * scale;
   }
+}
+
+// Headless ColorKernel (src/LatticeContainer.inc.cpp.Rt:350-412): one RGBA
+// byte quadruple per node of plane z, x fastest. The model's Color() gives
+// l = |U| (U as the quantity export computes it, from the pulled densities)
+// and a weight w; l * 111 goes through TCLB's piecewise-linear map (white /
+// cyan / blue for negative, red / yellow / white for positive values), w = 0
+// paints the node green and a non-finite l magenta. The arithmetic is float
+// with explicitly rounded operations, so a CPU restatement reproduces every
+// byte.
+__device__ __forceinline__ uchar4 color_map(float l, float w) {
+  int r = 0, g = 0, b = 0;
+  if (isfinite(l)) {
+    l = __fmul_rn(l, 111.f);
+    if (l < -111.f) { r = 255; g = 255; b = 255; }
+    else if (l < -11.f) { r = (int)__fdiv_rn(__fmul_rn(255.f, __fadd_rn(-l, -11.f)), 100.f); g = 255; b = 255; }
+    else if (l < -1.f) { r = 0; g = (int)__fdiv_rn(__fmul_rn(255.f, __fadd_rn(-l, -1.f)), 10.f); b = 255; }
+    else if (l < 0.f) { r = 0; g = 0; b = (int)__fmul_rn(255.f, -l); }
+    else if (l < 1.f) { r = (int)__fmul_rn(255.f, l); g = 0; b = 0; }
+    else if (l < 11.f) { r = 255; g = (int)__fdiv_rn(__fmul_rn(255.f, __fadd_rn(l, -1.f)), 10.f); b = 0; }
+    else if (l < 111.f) { r = 255; g = 255; b = (int)__fdiv_rn(__fmul_rn(255.f, __fadd_rn(l, -11.f)), 100.f); }
+    else { r = 255; g = 255; b = 255; }
+    r = (int)__fmul_rn((float)r, w);
+    g = (int)__fadd_rn(__fmul_rn((float)g, w), __fmul_rn(__fadd_rn(1.f, -w), 255.f));
+    b = (int)__fmul_rn((float)b, w);
+  } else {
+    r = 255; g = 0; b = 255;
+  }
+  return make_uchar4((unsigned char)r, (unsigned char)g, (unsigned char)b, 255);
+}
+
+template <class R>
+__device__ __forceinline__ float speed(const R* u, bool three) {
+  if constexpr (sizeof(R) == 8) {
+    double s = __dadd_rn(__dmul_rn(u[0], u[0]), __dmul_rn(u[1], u[1]));
+    if (three) s = __dadd_rn(s, __dmul_rn(u[2], u[2]));
+    return (float)sqrt(s);
+  } else {
+    float s = __fadd_rn(__fmul_rn(u[0], u[0]), __fmul_rn(u[1], u[1]));
+    if (three) s = __fadd_rn(s, __fmul_rn(u[2], u[2]));
+    return __fsqrt_rn(s);
+  }
+}
+
+template <class M, class R, class St>
+__global__ void k_color(const Args<R, M::NSET> a, int z, uchar4* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= a.nx || y >= a.ny) return;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int xm = (x == 0 ? nx : x) - 1, xp = (x + 1 == nx) ? 0 : x + 1;
+  const int ym = (y == 0 ? ny : y) - 1, yp = (y + 1 == ny) ? 0 : y + 1;
+  const int zm = (z == 0 ? nz : z) - 1, zp = (z + 1 == nz) ? 0 : z + 1;
+  const typename St::T* src = static_cast<const typename St::T*>(a.src);
+  R f[M::Q];
+#pragma unroll
+  for (int d = 0; d < M::Q; d++) {
+    const int sx = M::ex(d) == 0 ? x : (M::ex(d) > 0 ? xm : xp);
+    const int sy = M::ey(d) == 0 ? y : (M::ey(d) > 0 ? ym : yp);
+    const int sz = M::DIM == 2 ? z : (M::ez(d) == 0 ? z : (M::ez(d) > 0 ? zm : zp));
+    f[d] = St::template load<R>(src + (size_t)d * a.stride + (sx + nx * (sy + ny * sz)), R(M::w(d)));
+  }
+  const flag_t fl = a.flags[x + nx * (y + ny * z)];
+  R u[3];
+  M::template quantity<R>(1, f, fl, a, u);
+  out[x + (size_t)nx * y] = color_map(speed<R>(u, M::DIM == 3), M::color_weight(fl));
 }
 
 }  // namespace tclb

@@ -8,6 +8,7 @@
 // independent and any number of lattices can share a GPU.
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -163,6 +164,7 @@ struct Impl {
   void (*init)(tclb_lattice*, cudaStream_t);
   void (*quantity)(tclb_lattice*, int, int, const int*, double, void*, cudaStream_t);
   void (*equilibrium)(tclb_lattice*, const void*, const void*, cudaStream_t);
+  void (*color)(tclb_lattice*, int, void*, cudaStream_t);
   void (*to_double)(const void*, size_t, size_t, size_t, int, double*);   // storage -> double SoA
   void (*from_double)(const double*, size_t, size_t, size_t, int, void*);  // double SoA -> storage
   size_t real_size;
@@ -223,6 +225,10 @@ struct Launch {
     k_equilibrium<M, R, St><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, static_cast<const R*>(rho),
                                                                        static_cast<const R*>(u));
   }
+  static void color(tclb_lattice* L, int z, void* out, cudaStream_t s) {
+    auto a = make_args<M, R>(L, L->buf[L->cur], nullptr);
+    k_color<M, R, St><<<dim3((L->nx + 127) / 128, L->ny), 128, 0, s>>>(a, z, static_cast<uchar4*>(out));
+  }
   static void to_double(const void* raw, size_t N, size_t stride, size_t, int Q, double* out) {
     const typename St::T* p = static_cast<const typename St::T*>(raw);
     for (int q = 0; q < Q; q++)
@@ -234,7 +240,7 @@ struct Launch {
       for (size_t n = 0; n < N; n++) p[(size_t)q * stride + n] = St::from_double(in[(size_t)q * N + n], M::w(q));
   }
   static const Impl* get() {
-    static const Impl impl = {iterate, init, quantity, equilibrium, to_double, from_double, sizeof(R)};
+    static const Impl impl = {iterate, init, quantity, equilibrium, color, to_double, from_double, sizeof(R)};
     return &impl;
   }
 };
@@ -645,6 +651,32 @@ int tclb_get_quantity(tclb_h L, int q, const int region[6], void* out, double sc
   return TCLB_OK;
 }
 
+int tclb_color(tclb_h L, void* rgba, int z, int on_host, void* stream) {
+  CHECK_H(L);
+  if (!rgba) return fail(TCLB_ERR_ARG, "null output");
+  if (z < 0) z = L->nz / 2;  // LatticeContainer::Color draws plane nz/2
+  if (z >= L->nz) return fail(TCLB_ERR_ARG, "plane outside the lattice");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const size_t bytes = (size_t)L->nx * L->ny * 4;
+  if (!on_host) {
+    L->impl->color(L, z, rgba, s);
+    TCLB_CK(cudaGetLastError());
+    return TCLB_OK;
+  }
+  if (bytes > L->qbuf_bytes) {
+    if (L->qbuf) TCLB_CK(cudaFree(L->qbuf));
+    L->qbuf = nullptr;
+    L->qbuf_bytes = 0;
+    TCLB_CK(cudaMalloc(&L->qbuf, bytes));
+    L->qbuf_bytes = bytes;
+  }
+  L->impl->color(L, z, L->qbuf, s);
+  TCLB_CK(cudaGetLastError());
+  TCLB_CK(cudaMemcpyAsync(rgba, L->qbuf, bytes, cudaMemcpyDeviceToHost, s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
 int tclb_get_densities(tclb_h L, double* out) {
   CHECK_H(L);
   if (!out) return fail(TCLB_ERR_ARG, "null output");
@@ -706,11 +738,22 @@ int tclb_load(tclb_h L, const void* host, size_t bytes, void* stream) {
 // TCLB's .pri snapshot (Lattice::save / load, src/Lattice.cu.Rt:642-769): the
 // non-empty margin blocks of a snapshot, block k = 1..27 with offsets
 // (dx,dy,dz) = ((k-1)%3-1, ((k-1)/3)%3-1, (k-1)/9-1), concatenated. Block
-// (0,0,0) is the interior; a margin block holds, for every density that is
-// pulled across that face/edge/corner, the values its ghost layer carries --
-// on one rank the wrapped values of the opposite side -- as an x-fastest box
-// (src/conf.R:771-1023 with the default GPU layout). Fields are in density
-// order, values in storage_t.
+// (0,0,0) is the interior. Density i (velocity e) is a field spanning
+// offsets -e (src/conf.R:65-100, AddDensity -> AddField(dx=-dx)), so it owns
+// a box in every block d with d_a in {0, -e_a} on each axis; boxes are
+// x-fastest, fields in density order within a block, values in storage_t
+// (src/conf.R:905-1000, default GPU layout: no X_MOD, no CPU layout).
+//
+// Where a node's value is written (the put of src/conf.R:978-983 driven by
+// if.apply in src/LatticeAccess.inc.cpp.Rt:83-117): a node on the outgoing
+// edge of axis a (e_a = +1 at n_a-1, e_a = -1 at 0) writes density i into
+// the margin d_a = -e_a at position 0; every other node writes it in place.
+// Models that also register the densities as unshifted fields (d3q27_cumulant,
+// models/flow/d3q27_cumulant/Dynamics.R:51) write the edge node in place too,
+// so their interior is complete; in d2q9 and d3q19 those interior slots are
+// never written and stay zero (the snapshot is zeroed at allocation,
+// src/LatticeContainer.inc.cpp.Rt:119). On one rank the margin d_a = -1
+// is what node 0 pulls: the periodic wrap.
 // ---------------------------------------------------------------------------
 namespace {
 struct PriBlock {
@@ -719,39 +762,84 @@ struct PriBlock {
   int n[3];
 };
 
+struct PriLayout {
+  std::vector<PriBlock> blocks;
+  std::vector<std::array<int, 3>> e;  // velocity of each density
+  bool interior_copy;                 // edge nodes also written in place
+  int dims[3];
+
+  // true when slot (block b, density i, node n) is written by node n's put
+  bool written(const PriBlock& b, int i, const int* n) const {
+    for (int a = 0; a < 3; a++) {
+      if (b.d[a] != 0) continue;
+      const bool outgoing = (e[i][a] == 1 && n[a] == dims[a] - 1) || (e[i][a] == -1 && n[a] == 0);
+      if (outgoing && !interior_copy) return false;
+    }
+    return true;
+  }
+  // true when block b is where node n's density i is pulled from
+  bool primary(const PriBlock& b, int i, const int* n) const {
+    for (int a = 0; a < 3; a++) {
+      const bool outgoing = (e[i][a] == 1 && n[a] == dims[a] - 1) || (e[i][a] == -1 && n[a] == 0);
+      if (b.d[a] != (outgoing ? -e[i][a] : 0)) return false;
+    }
+    return true;
+  }
+};
+
 template <class M>
-std::vector<PriBlock> pri_blocks_m(int nx, int ny, int nz) {
-  std::vector<PriBlock> out;
-  const int dims[3] = {nx, ny, nz};
+PriLayout pri_layout_m(int nx, int ny, int nz, bool interior_copy) {
+  PriLayout L;
+  L.dims[0] = nx;
+  L.dims[1] = ny;
+  L.dims[2] = nz;
+  L.interior_copy = interior_copy;
+  for (int i = 0; i < M::Q; i++) L.e.push_back({M::ex(i), M::ey(i), M::ez(i)});
   for (int k = 0; k < 27; k++) {
     PriBlock b;
     b.d[0] = k % 3 - 1;
     b.d[1] = (k / 3) % 3 - 1;
     b.d[2] = k / 9 - 1;
     for (int i = 0; i < M::Q; i++) {
-      const int e[3] = {M::ex(i), M::ey(i), M::ez(i)};
       bool in = true;
-      for (int a = 0; a < 3; a++) in = in && (b.d[a] == 0 || e[a] == -b.d[a]);  // pulled across this side
+      for (int a = 0; a < 3; a++) in = in && (b.d[a] == 0 || L.e[i][a] == -b.d[a]);
       if (in) b.fields.push_back(i);
     }
-    for (int a = 0; a < 3; a++) b.n[a] = b.d[a] == 0 ? dims[a] : 1;
-    if (!b.fields.empty()) out.push_back(b);
+    for (int a = 0; a < 3; a++) b.n[a] = b.d[a] == 0 ? L.dims[a] : 1;
+    if (!b.fields.empty()) L.blocks.push_back(b);
   }
-  return out;
+  return L;
 }
 
-std::vector<PriBlock> pri_blocks(const tclb_lattice* L) {
+PriLayout pri_layout(const tclb_lattice* L) {
   switch (L->model) {
-    case MODEL_D2Q9: return pri_blocks_m<D2Q9>(L->nx, L->ny, L->nz);
-    case MODEL_D3Q19: return pri_blocks_m<D3Q19>(L->nx, L->ny, L->nz);
-    default: return pri_blocks_m<D3Q27C>(L->nx, L->ny, L->nz);
+    case MODEL_D2Q9: return pri_layout_m<D2Q9>(L->nx, L->ny, L->nz, false);
+    case MODEL_D3Q19: return pri_layout_m<D3Q19>(L->nx, L->ny, L->nz, false);
+    default: return pri_layout_m<D3Q27C>(L->nx, L->ny, L->nz, true);
   }
 }
 
 size_t pri_size(const tclb_lattice* L) {
   size_t s = 0;
-  for (const auto& b : pri_blocks(L)) s += b.fields.size() * (size_t)b.n[0] * b.n[1] * b.n[2] * L->elem;
+  for (const auto& b : pri_layout(L).blocks) s += b.fields.size() * (size_t)b.n[0] * b.n[1] * b.n[2] * L->elem;
   return s;
+}
+
+// Calls f(block, density, node, byte offset in the file) for every slot.
+template <class F>
+void pri_for_each(const tclb_lattice* L, const PriLayout& P, F&& f) {
+  size_t off = 0;
+  for (const auto& b : P.blocks)
+    for (int i : b.fields)
+      for (int z = 0; z < b.n[2]; z++)
+        for (int y = 0; y < b.n[1]; y++)
+          for (int x = 0; x < b.n[0]; x++) {
+            const int p[3] = {x, y, z};
+            int n[3];
+            for (int a = 0; a < 3; a++) n[a] = b.d[a] < 0 ? P.dims[a] - 1 : (b.d[a] > 0 ? 0 : p[a]);
+            f(b, i, n, off);
+            off += L->elem;
+          }
 }
 }  // namespace
 
@@ -767,19 +855,15 @@ int tclb_save_pri(tclb_h L, void* host, size_t bytes) {
   TCLB_CK(cudaStreamSynchronize(L->stream));
   char* o = static_cast<char*>(host);
   const size_t e = L->elem;
-  for (const auto& b : pri_blocks(L))
-    for (int i : b.fields)
-      for (int z = 0; z < b.n[2]; z++)
-        for (int y = 0; y < b.n[1]; y++)
-          for (int x = 0; x < b.n[0]; x++) {
-            // ghost at -1 carries the value of the last layer, ghost at +n the first
-            const int sx = b.d[0] < 0 ? L->nx - 1 : (b.d[0] > 0 ? 0 : x);
-            const int sy = b.d[1] < 0 ? L->ny - 1 : (b.d[1] > 0 ? 0 : y);
-            const int sz = b.d[2] < 0 ? L->nz - 1 : (b.d[2] > 0 ? 0 : z);
-            const size_t n = (size_t)sx + (size_t)L->nx * ((size_t)sy + (size_t)L->ny * sz);
-            std::memcpy(o, raw.data() + ((size_t)i * L->stride + n) * e, e);
-            o += e;
-          }
+  const PriLayout P = pri_layout(L);
+  pri_for_each(L, P, [&](const PriBlock& b, int i, const int* n, size_t off) {
+    if (P.written(b, i, n)) {
+      const size_t node = (size_t)n[0] + (size_t)L->nx * ((size_t)n[1] + (size_t)L->ny * n[2]);
+      std::memcpy(o + off, raw.data() + ((size_t)i * L->stride + node) * e, e);
+    } else {
+      std::memset(o + off, 0, e);
+    }
+  });
   return TCLB_OK;
 }
 
@@ -789,17 +873,12 @@ int tclb_load_pri(tclb_h L, const void* host, size_t bytes) {
   const char* in = static_cast<const char*>(host);
   const size_t e = L->elem;
   std::vector<char> raw(L->stride * L->T->Q * L->elem, 0);
-  for (const auto& b : pri_blocks(L)) {
-    const size_t box = (size_t)b.n[0] * b.n[1] * b.n[2];
-    if (b.d[0] == 0 && b.d[1] == 0 && b.d[2] == 0) {  // the interior carries the state
-      for (int i : b.fields) {
-        std::memcpy(raw.data() + (size_t)i * L->stride * e, in, box * e);
-        in += box * e;
-      }
-    } else {
-      in += b.fields.size() * box * e;
-    }
-  }
+  const PriLayout P = pri_layout(L);
+  pri_for_each(L, P, [&](const PriBlock& b, int i, const int* n, size_t off) {
+    if (!P.primary(b, i, n)) return;  // each node's value is taken from the block it is pulled from
+    const size_t node = (size_t)n[0] + (size_t)L->nx * ((size_t)n[1] + (size_t)L->ny * n[2]);
+    std::memcpy(raw.data() + ((size_t)i * L->stride + node) * e, in + off, e);
+  });
   TCLB_CK(cudaMemcpyAsync(L->buf[L->cur], raw.data(), raw.size(), cudaMemcpyHostToDevice, L->stream));
   TCLB_CK(cudaStreamSynchronize(L->stream));
   return TCLB_OK;

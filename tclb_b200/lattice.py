@@ -76,6 +76,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_pri_bytes.restype = sz
     L.tclb_save_pri.argtypes = [h, vp, sz]
     L.tclb_load_pri.argtypes = [h, vp, sz]
+    L.tclb_color.argtypes = [h, vp, i, i, vp]
     _lib = L
     return L
 
@@ -231,6 +232,21 @@ class Lattice:
         n = self.snapshot_bytes()
         ptr = buf.ctypes.data if hasattr(buf, "ctypes") else buf
         _check(self.lib.tclb_load(self._h, ctypes.c_void_p(ptr), n, ctypes.c_void_p(stream or None)))
+
+    def Color(self, z: int = -1, device_ptr: Optional[int] = None, stream: int = 0) -> Optional[np.ndarray]:
+        """Lattice::Color, headless: RGBA bytes (ny, nx, 4) of plane z (default
+        nz/2). With device_ptr the bytes go to that device buffer on `stream`
+        and nothing is returned."""
+        if device_ptr is not None:
+            _check(self.lib.tclb_color(self._h, ctypes.c_void_p(device_ptr), int(z), 0,
+                                       ctypes.c_void_p(stream or None)))
+            return None
+        out = np.zeros((self.ny, self.nx, 4), np.uint8)
+        _check(self.lib.tclb_color(self._h, ctypes.c_void_p(out.ctypes.data), int(z), 1,
+                                   ctypes.c_void_p(stream or None)))
+        return out
+
+    color = Color
 
     def save_pri(self) -> np.ndarray:
         """TCLB's .pri layout of the current snapshot (margin blocks concatenated)."""
