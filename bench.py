@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--pairs", type=int, default=1,
+                   help="0 = one node per thread also for 16-bit storage (default 1: two nodes per "
+                        "thread when nx is a multiple of 64)")
     p.add_argument("--config", type=int, default=2,
                    help="2 = the headline Taylor-Green line; 1, 3, 4, 5 = the other configurations (one JSON line)")
     return p.parse_args()
@@ -139,8 +142,17 @@ def profiled_traffic(model, precision, storage, n):
 
 
 # ---------------------------------------------------------------------------
-def tgv_setup(lat, n, u0=0.05, nu=1e-3):
+# Taylor-Green viscosity per model: 1e-3 is the d3q27_cumulant configuration;
+# the d3q19 MRT (omega = 1.988 at nu = 1e-3) diverges on this under-resolved
+# flow, so its throughput lines run the stable nu = 1e-2.
+TGV_NU = {"d3q27_cumulant": 1e-3, "d3q19": 1e-2, "d2q9": 1e-2}
+
+
+def tgv_setup(lat, n, u0=0.05, nu=None):
     from tclb_b200 import cases
+
+    if nu is None:
+        nu = TGV_NU[lat.model.name]
 
     lat.set_flags(cases.tgv_flags(lat.model, n, nz=lat.nz))
     lat.SetSetting("nu", nu)
@@ -159,7 +171,7 @@ def cpu_baseline(args, model_name, seconds, threads=None):
     n, nz = args.n, args.cpu_slab
     o = oracle.OracleLattice(model_name, n, n, nz, precision=args.precision if args.precision == "fp64" else "fp32")
     o.set_flags(cases.tgv_flags(model_name, n, nz=nz))
-    o.set_setting("nu", 1e-3)
+    o.set_setting("nu", TGV_NU[model_name])
     m = M.get(model_name)
     rho, u = cases.tgv_fields(n, u0=0.05, nz=nz, dtype=np.float64)
     J = rho[..., None] * u
@@ -252,6 +264,8 @@ def run_ours(args):
         cpu = cpu_baseline(args, args.model, args.cpu_seconds)
 
     lat = Lattice(args.model, n, n, n, precision=args.precision, storage=args.storage)
+    if not args.pairs:
+        lat.set_launch(128 if n >= 128 else 32, 2 if n >= 128 else 8, use_graphs=True, use_pairs=False)
     tgv_setup(lat, n)
     # a dedicated (non-default) stream: the library launches on it, the CUDA
     # events below are recorded on it
@@ -336,11 +350,12 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-                "config": {"workload": f"{args.model} Taylor-Green vortex {n}^3 periodic, u0=0.05, nu=1e-3",
+                "config": {"workload": f"{args.model} Taylor-Green vortex {n}^3 periodic, u0=0.05, "
+                                       f"nu={TGV_NU[args.model]:g}",
                            "model": args.model, "lattice": [n, n, n], "precision": args.precision,
                            "storage": args.storage, "iterations_per_step": I, "globals_every": I,
                            "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % (bpu / 2 * N / 1e9),
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}", "two_nodes_per_thread": bool(args.pairs) and args.storage != "same" and n % 64 == 0},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": args.steps * I, "wall_s": wall,
                 "globals_last": {k: float(v) for k, v in glob.items()}}

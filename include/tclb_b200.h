@@ -171,9 +171,9 @@ int tclb_sync(tclb_h h);
 /* Launch shape of the iteration kernel (bx multiple of 32, bx*by <= 256) and
    flags: TCLB_LAUNCH_GRAPHS replays runs of plain iterations from a captured
    CUDA graph (on by default); TCLB_LAUNCH_PAIRS lets 16-bit storage with
-   nx % 64 == 0 update two nodes per thread with 32-bit accesses (off by
-   default: its register use halves the occupancy, which costs more than the
-   wider accesses gain on B200). */
+   nx % 64 == 0 update two nodes per thread on plain iterations: 32-bit
+   accesses, and for d3q19 / d3q27_cumulant bulk nodes one packed FP32x2
+   collision for both (on by default). bx, by shape the one-node kernel. */
 #define TCLB_LAUNCH_GRAPHS 1
 #define TCLB_LAUNCH_PAIRS 2
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);

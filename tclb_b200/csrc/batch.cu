@@ -59,6 +59,7 @@ Args<R, M::NSET> args_of(const BatchCase& C, const void* src, void* dst) {
   a.zone = static_cast<const R*>(C.zone);
   a.glob = C.glob;
   for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
+  M::template derived<R>(a.s, a.k);
   return a;
 }
 

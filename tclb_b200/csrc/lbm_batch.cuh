@@ -74,20 +74,23 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
         a.glob = C.glob;
 #pragma unroll
         for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
+        M::template derived<R>(a.s, a.k);
       }
       if (skip) continue;
       const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
       const bool act = x < a.nx && y < a.ny;
+      using T = typename St::T;
+      const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
       if (k == last) {
         R g[M::NG];
 #pragma unroll
         for (int i = 0; i < M::NG; i++) g[i] = 0;
-        if (act) node_update<M, R, St, true>(a, x, y, z, g);
+        if (act) node_update<M, R, St, true>(a, P, x, y, z, g);
         reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
         __syncthreads();  // shared scratch of reduce_globals reused by the next tile
       } else if (act) {
         R g[1];
-        node_update<M, R, St, false>(a, x, y, z, g);
+        node_update<M, R, St, false>(a, P, x, y, z, g);
       }
     }
   }

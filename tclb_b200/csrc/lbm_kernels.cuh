@@ -14,6 +14,7 @@
 
 #include <cstdint>
 
+#include "f32x2.cuh"
 #include "tclb_models.h"
 
 namespace tclb {
@@ -91,6 +92,7 @@ struct Args {
   const R* zone;  // [zones][NZS] zonal settings
   double* glob;   // device Globals (FP64)
   R s[NSET];      // settings
+  R k[4];         // per-launch constants derived from the settings (Model::derived)
 };
 
 // AddTo<Global>(x) with TCLB's Objective rule: every AddTo of a SUM Global
@@ -108,6 +110,13 @@ __device__ __forceinline__ void add_glob(R* g, int i, R x, const R* zs) {
 struct D2Q9 {
   static constexpr int Q = 9, DIM = 2, NSET = d2q9::NSET, NZS = d2q9::NZS, NG = d2q9::NG, NSUM = d2q9::NSUM,
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
+  static constexpr bool has_bulk = false;  // no packed two-node collision
+  static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 1;
+  __device__ __forceinline__ static bool bulk(flag_t) { return false; }
+  template <class V, class R>
+  __device__ __forceinline__ static void collide_bulk(V (&)[Q], const Args<R, NSET>&) {}
+  template <class R>
+  __host__ __device__ static void derived(const R*, R* k) { k[0] = k[1] = k[2] = k[3] = R(0); }
   __host__ __device__ static constexpr int ex(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0); }
   __host__ __device__ static constexpr int ey(int i) { return (i == 2 || i == 5 || i == 6) ? 1 : ((i == 4 || i == 7 || i == 8) ? -1 : 0); }
   __host__ __device__ static constexpr int ez(int) { return 0; }
@@ -275,6 +284,17 @@ struct D2Q9 {
 struct D3Q19 {
   static constexpr int Q = 19, DIM = 3, NSET = d3q19::NSET, NZS = d3q19::NZS, NG = d3q19::NG, NSUM = d3q19::NSUM,
                        ZONE_SHIFT = d3q19::ZONE_SHIFT;
+  static constexpr bool has_bulk = true;
+  // two-node kernel: 256 threads, <= 80 registers (3 blocks per SM), no spills
+  static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 3;
+  // gamma1 = 1 - omega and gamma2 = 1 - 8(2 - omega)/(8 - omega), once per launch
+  template <class R>
+  __host__ __device__ static void derived(const R* s, R* k) {
+    const R omega = s[d3q19::S_omega];
+    k[0] = R(1) - omega;
+    k[1] = R(1) - R(8) * (R(2) - omega) / (R(8) - omega);
+    k[2] = k[3] = R(0);
+  }
   // directions: columns 4, 6, 8 of MRTMAT (d3q19/Dynamics.R:26-35)
   __host__ __device__ static constexpr int ex(int i) {
     return (i == 1 || i == 7 || i == 9 || i == 11 || i == 13) ? 1 : ((i == 2 || i == 8 || i == 10 || i == 12 || i == 14) ? -1 : 0);
@@ -385,37 +405,53 @@ struct D3Q19 {
   //   f_i <- feq_i(J') + gamma1 (f - feq(J))_i^even + gamma2 (f - feq(J))_i^odd
   // with even/odd parts taken over each pair (i, opposite i). It is evaluated
   // that way here: pair sums and differences instead of two 19x19 transforms.
-  template <class R, bool G>
-  __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
-    R s[9], d[9];
+  // The two-rate update for value type V (R, or F2 for two nodes); leaves
+  // rho and the forced momentum J' for the Globals.
+  template <class V, class R>
+  __device__ __forceinline__ static void trt(V (&f)[Q], const Args<R, NSET>& a, V& rho, V& jx, V& jy, V& jz) {
+    V s[9], d[9];
 #pragma unroll
     for (int p = 0; p < 9; p++) {
       s[p] = f[pair_a(p)] + f[pair_b(p)];
       d[p] = f[pair_a(p)] - f[pair_b(p)];
     }
-    const R rho = f[0] + (s[0] + s[1] + s[2]) + ((s[3] + s[4]) + (s[5] + s[6]) + (s[7] + s[8]));
-    R jx = d[0] + d[3] - d[4] + d[5] - d[6];
-    R jy = d[1] + d[3] + d[4] + d[7] - d[8];
-    R jz = d[2] + d[5] + d[6] + d[7] + d[8];
-    const R omega = a.s[d3q19::S_omega];
-    const R g1 = R(1) - omega;
-    const R g2 = R(1) - R(8) * (R(2) - omega) / (R(8) - omega);
-    const R irho = R(1) / rho;
-    R e0, e[9], o[9];
+    rho = f[0] + (s[0] + s[1] + s[2]) + ((s[3] + s[4]) + (s[5] + s[6]) + (s[7] + s[8]));
+    jx = d[0] + d[3] - d[4] + d[5] - d[6];
+    jy = d[1] + d[3] + d[4] + d[7] - d[8];
+    jz = d[2] + d[5] + d[6] + d[7] + d[8];
+    const V g1 = V(a.k[0]), g2 = V(a.k[1]);
+    const V irho = recip(rho);
+    V e0, e[9], o[9];
     feq_parts(rho, irho, jx, jy, jz, e0, e, o);
-    jx += rho * a.s[d3q19::S_ForceX];
-    jy += rho * a.s[d3q19::S_ForceY];
-    jz += rho * a.s[d3q19::S_ForceZ];
-    R e0n, en[9], on[9];
+    jx += rho * V(a.s[d3q19::S_ForceX]);
+    jy += rho * V(a.s[d3q19::S_ForceY]);
+    jz += rho * V(a.s[d3q19::S_ForceZ]);
+    V e0n, en[9], on[9];
     feq_parts(rho, irho, jx, jy, jz, e0n, en, on);
     f[0] = e0n + g1 * (f[0] - e0);
 #pragma unroll
     for (int p = 0; p < 9; p++) {
-      const R E = en[p] + g1 * (R(0.5) * s[p] - e[p]);
-      const R O = on[p] + g2 * (R(0.5) * d[p] - o[p]);
+      const V E = en[p] + g1 * (V(0.5) * s[p] - e[p]);
+      const V O = on[p] + g2 * (V(0.5) * d[p] - o[p]);
       f[pair_a(p)] = E + O;
       f[pair_b(p)] = E - O;
     }
+  }
+
+  // A node with no boundary type and the MRT collision, without Globals.
+  __device__ __forceinline__ static bool bulk(flag_t fl) {
+    return (fl & d3q19::BOUNDARY) == 0 && (fl & d3q19::COLLISION) == d3q19::MRT;
+  }
+  template <class V, class R>
+  __device__ __forceinline__ static void collide_bulk(V (&f)[Q], const Args<R, NSET>& a) {
+    V rho, jx, jy, jz;
+    trt(f, a, rho, jx, jy, jz);
+  }
+
+  template <class R, bool G>
+  __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
+    R rho, jx, jy, jz;
+    trt(f, a, rho, jx, jy, jz);
     if (G) {  // :266-289, with rho and J already divided by Mw = 19, 10 (C(R, Mw, eq="/="))
       const R rs = rho * R(1.0 / 19.0), px = jx * R(0.1), py = jy * R(0.1), pz = jz * R(0.1);
       const R ux = px / rs, uy = py / rs, uz = pz / rs;
@@ -534,6 +570,16 @@ struct D3Q19 {
 struct D3Q27C {
   static constexpr int Q = 27, DIM = 3, NSET = d3q27c::NSET, NZS = d3q27c::NZS, NG = d3q27c::NG,
                        NSUM = d3q27c::NSUM, ZONE_SHIFT = d3q27c::ZONE_SHIFT;
+  static constexpr bool has_bulk = true;
+  // two-node kernel: 128 threads, <= 96 registers (5 blocks per SM), no spills
+  static constexpr int PAIR_THREADS = 128, PAIR_MIN_BLOCKS = 5;
+  // relaxation rates of the bulk (nu) and of BOUNDARY nodes (nubuffer), once per launch
+  template <class R>
+  __host__ __device__ static void derived(const R* s, R* k) {
+    k[0] = R(1) / (R(3) * s[d3q27c::S_nu] + R(0.5));
+    k[1] = R(1) / (R(3) * s[d3q27c::S_nubuffer] + R(0.5));
+    k[2] = k[3] = R(0);
+  }
   // f<a><b><c>: index a + 3b + 9c, digit 0 -> 0, 1 -> +1, 2 -> -1
   __host__ __device__ static constexpr int dg(int v) { return v == 1 ? 1 : (v == 2 ? -1 : 0); }
   __host__ __device__ static constexpr int ex(int i) { return dg(i % 3); }
@@ -647,17 +693,8 @@ struct D3Q27C {
   template <class R, bool G>
   __device__ __forceinline__ static void collide(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
     const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
-    const R w0 = (fl & d3q27c::BOUNDARY) ? R(1) / (R(3) * a.s[d3q27c::S_nubuffer] + R(0.5))
-                                         : R(1) / (R(3) * a.s[d3q27c::S_nu] + R(0.5));
-    // raw moments: x, y, z passes
-#pragma unroll
-    for (int r = 0; r < 27; r += 3) raw3(f[r], f[r + 1], f[r + 2]);
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-#pragma unroll
-      for (int x = 0; x < 3; x++) raw3(f[x + 9 * c], f[x + 3 + 9 * c], f[x + 6 + 9 * c]);
-#pragma unroll
-    for (int r = 0; r < 9; r++) raw3(f[r], f[r + 9], f[r + 18]);
+    const R w0 = (fl & d3q27c::BOUNDARY) ? a.k[1] : a.k[0];
+    to_raw(f);
     if (G) {  // :311-319 with getU_ (:30-45); rho and J are the raw moments m000, m100, m010, m001
       const R rho = f[0], jx = f[1], jy = f[3], jz = f[9];
       R ux = (jx + Fx / R(2)) / rho, uy = (jy + Fy / R(2)) / rho, uz = (jz + Fz / R(2)) / rho;
@@ -672,9 +709,25 @@ struct D3Q27C {
     // Cumulants of order >= 4 are set to zero by the collision and those of
     // order 3 are scaled by (1 - Omega): with the default Omega = 1 they vanish
     // too, so only orders <= 2 are converted (a branch uniform over the launch).
-    if (a.s[d3q27c::S_Omega] == R(1)) relax<R, false>(f, a, w0);
-    else relax<R, true>(f, a, w0);
-    // back to populations: x, y, z passes
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<R, R, false>(f, a, w0);
+    else relax<R, R, true>(f, a, w0);
+    from_raw(f);
+  }
+
+  // populations -> raw moments (x, y, z passes) and back
+  template <class V>
+  __device__ __forceinline__ static void to_raw(V (&f)[Q]) {
+#pragma unroll
+    for (int r = 0; r < 27; r += 3) raw3(f[r], f[r + 1], f[r + 2]);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) raw3(f[x + 9 * c], f[x + 3 + 9 * c], f[x + 6 + 9 * c]);
+#pragma unroll
+    for (int r = 0; r < 9; r++) raw3(f[r], f[r + 9], f[r + 18]);
+  }
+  template <class V>
+  __device__ __forceinline__ static void from_raw(V (&f)[Q]) {
 #pragma unroll
     for (int r = 0; r < 27; r += 3) unraw3(f[r], f[r + 1], f[r + 2]);
 #pragma unroll
@@ -685,39 +738,52 @@ struct D3Q27C {
     for (int r = 0; r < 9; r++) unraw3(f[r], f[r + 9], f[r + 18]);
   }
 
+  // A node with no boundary type or extra group and the MRT collision,
+  // without Globals; V = R, or F2 for two nodes.
+  __device__ __forceinline__ static bool bulk(flag_t fl) {
+    return (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) == 0 && (fl & d3q27c::COLLISION) == d3q27c::MRT;
+  }
+  template <class V, class R>
+  __device__ __forceinline__ static void collide_bulk(V (&f)[Q], const Args<R, NSET>& a) {
+    to_raw(f);
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<V, R, false>(f, a, V(a.k[0]));
+    else relax<V, R, true>(f, a, V(a.k[0]));
+    from_raw(f);
+  }
+
   // Raw moments f -> cumulants -> relaxed cumulants -> raw moments (:359-477).
-  template <class R, bool THIRD>
-  __device__ __forceinline__ static void relax(R (&f)[Q], const Args<R, NSET>& a, R w0) {
-    const R Fx = a.s[d3q27c::S_ForceX], Fy = a.s[d3q27c::S_ForceY], Fz = a.s[d3q27c::S_ForceZ];
-    const R w1 = R(1);
-    R c[Q];
-    const R m0 = f[0], im0 = R(1) / m0;
+  template <class V, class R, bool THIRD>
+  __device__ __forceinline__ static void relax(V (&f)[Q], const Args<R, NSET>& a, V w0) {
+    const V Fx = V(a.s[d3q27c::S_ForceX]), Fy = V(a.s[d3q27c::S_ForceY]), Fz = V(a.s[d3q27c::S_ForceZ]);
+    const V w1 = V(1);
+    V c[Q];
+    const V m0 = f[0], im0 = recip(m0);
     if (THIRD) cum_from_raw_o3(f, c, im0);
     else cum_from_raw_o2(f, c, im0);
-    // relaxation (:386-449)
-    const R ux = c[1] + Fx * R(0.5) * im0, uy = c[3] + Fy * R(0.5) * im0, uz = c[9] + Fz * R(0.5) * im0;
-    const R c200 = c[2], c020 = c[6], c002 = c[18];
-    const R dxu = -w0 / R(2) * (R(2) * c200 - c020 - c002) - w1 / R(2) * (c200 + c020 + c002 - R(1));
-    const R dyv = dxu + R(3) * w0 / R(2) * (c200 - c020);
-    const R dzw = dxu + R(3) * w0 / R(2) * (c200 - c002);
-    const R gcor1 = R(3) * (R(1) - w0 / R(2)) * (ux * ux * dxu - uy * uy * dyv);
-    const R gcor2 = R(3) * (R(1) - w0 / R(2)) * (ux * ux * dxu - uz * uz * dzw);
-    const R gcor3 = R(3) * (R(1) - w1 / R(2)) * (ux * ux * dxu + uy * uy * dyv + uz * uz * dzw);
-    const R GC = a.s[d3q27c::S_GalileanCorrection];
-    const R A = (R(1) - w0) * (c200 - c020) - gcor1 * GC;
-    const R B = (R(1) - w0) * (c200 - c002) - gcor2 * GC;
-    const R CC = w1 + (R(1) - w1) * (c200 + c020 + c002) - gcor3 * GC;
+    // relaxation (:386-449); x/2 written as x*0.5 (exact)
+    const V ux = c[1] + Fx * V(0.5) * im0, uy = c[3] + Fy * V(0.5) * im0, uz = c[9] + Fz * V(0.5) * im0;
+    const V c200 = c[2], c020 = c[6], c002 = c[18];
+    const V dxu = -w0 * V(0.5) * (V(2) * c200 - c020 - c002) - w1 * V(0.5) * (c200 + c020 + c002 - V(1));
+    const V dyv = dxu + V(3) * w0 * V(0.5) * (c200 - c020);
+    const V dzw = dxu + V(3) * w0 * V(0.5) * (c200 - c002);
+    const V gcor1 = V(3) * (V(1) - w0 * V(0.5)) * (ux * ux * dxu - uy * uy * dyv);
+    const V gcor2 = V(3) * (V(1) - w0 * V(0.5)) * (ux * ux * dxu - uz * uz * dzw);
+    const V gcor3 = V(3) * (V(1) - w1 * V(0.5)) * (ux * ux * dxu + uy * uy * dyv + uz * uz * dzw);
+    const V GC = V(a.s[d3q27c::S_GalileanCorrection]);
+    const V A = (V(1) - w0) * (c200 - c020) - gcor1 * GC;
+    const V B = (V(1) - w0) * (c200 - c002) - gcor2 * GC;
+    const V CC = w1 + (V(1) - w1) * (c200 + c020 + c002) - gcor3 * GC;
     c[1] += Fx;
-    c[2] = (A + B + CC) / R(3);
-    c[6] = (CC - R(2) * A + B) / R(3);
-    c[18] = (CC - R(2) * B + A) / R(3);
+    c[2] = (A + B + CC) * V(1.0 / 3.0);
+    c[6] = (CC - V(2) * A + B) * V(1.0 / 3.0);
+    c[18] = (CC - V(2) * B + A) * V(1.0 / 3.0);
     c[3] += Fy;
     c[9] += Fz;
-    c[4] *= (R(1) - w0);
-    c[12] *= (R(1) - w0);
-    c[10] *= (R(1) - w0);
+    c[4] *= (V(1) - w0);
+    c[12] *= (V(1) - w0);
+    c[10] *= (V(1) - w0);
     if (THIRD) {
-      const R om3 = R(1) - a.s[d3q27c::S_Omega];
+      const V om3 = V(R(1) - a.s[d3q27c::S_Omega]);
 #pragma unroll
       for (int n = 1; n < Q; n++)
         if (n % 3 + (n / 3) % 3 + n / 9 == 3) c[n] = om3 * c[n];
@@ -811,36 +877,76 @@ __device__ __forceinline__ void reduce_globals(const R (&g)[NG], double* out) {
 // ---------------------------------------------------------------------------
 // The fused iteration kernel: one thread per node.
 // ---------------------------------------------------------------------------
-// One node: pull from a.src with periodic wrap, run the model, store to a.dst.
+// Where the population planes are. StrideAddr derives plane i from one base
+// pointer and the plane stride (the batch kernel, whose case descriptors are
+// read from device memory); PlaneAddr carries all 2*Q plane base pointers as
+// a kernel parameter, so each load or store needs only its 32-bit node index
+// scaled onto a base that every thread shares.
+template <class T>
+struct StrideAddr {
+  static constexpr bool per_plane = false;
+  const T* s;
+  T* d;
+  size_t stride;
+  __device__ __forceinline__ const T* src(int i) const { return s + (size_t)i * stride; }
+  __device__ __forceinline__ T* dst(int i) const { return d + (size_t)i * stride; }
+};
+template <class T, int Q>
+struct PlaneAddr {
+  static constexpr bool per_plane = true;
+  const T* s[Q];
+  T* d[Q];
+  __device__ __forceinline__ const T* src(int i) const { return s[i]; }
+  __device__ __forceinline__ T* dst(int i) const { return d[i]; }
+};
+
+// One node: pull from the source planes with periodic wrap, run the model,
+// store to the destination planes.
 //
 // Addressing: the source of population i is node - e_i with periodic wrap.
 // Per axis the two possible offsets (pulling from the lower / upper
 // neighbour, wrapped at the faces) are computed once; each population's
-// offset is then the sum of three of them, chosen at compile time, and the
-// population planes are reached by adding the plane stride to one pointer.
-template <class M, class R, class St, bool G>
-__device__ __forceinline__ void node_update(const Args<R, M::NSET>& a, int x, int y, int z, R* g) {
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int sxy = nx * ny;
-  const int node = x + nx * y + sxy * z;
-  const int ox_lo = x == 0 ? nx - 1 : -1, ox_hi = x + 1 == nx ? 1 - nx : 1;                // e_x = +1 / -1
-  const int oy_lo = y == 0 ? nx * (ny - 1) : -nx, oy_hi = y + 1 == ny ? nx * (1 - ny) : nx;  // e_y = +1 / -1
-  const int oz_lo = z == 0 ? sxy * (nz - 1) : -sxy, oz_hi = z + 1 == nz ? sxy * (1 - nz) : sxy;
-  const typename St::T* __restrict__ src = static_cast<const typename St::T*>(a.src) + node;
-  typename St::T* __restrict__ dst = static_cast<typename St::T*>(a.dst) + node;
-  const size_t stride = a.stride;
+// offset is then the sum of three of them, chosen at compile time. Node
+// indices are unsigned 32-bit (a lattice has fewer than 2^32 nodes); a
+// negative offset wraps modulo 2^32 and lands on the right node.
+template <class M, class R, class St, bool G, class A>
+__device__ __forceinline__ void node_update(const Args<R, M::NSET>& a, const A& P, int x, int y, int z, R* g) {
+  const unsigned nx = a.nx, ny = a.ny, nz = a.nz;
+  const unsigned sxy = nx * ny;
+  const unsigned node = x + nx * y + sxy * z;
+  const unsigned ox_lo = x == 0 ? nx - 1 : 0u - 1u, ox_hi = x + 1 == (int)nx ? 1u - nx : 1u;  // e_x = +1 / -1
+  const unsigned oy_lo = y == 0 ? nx * (ny - 1) : 0u - nx, oy_hi = y + 1 == (int)ny ? nx * (1u - ny) : nx;
+  const unsigned oz_lo = z == 0 ? sxy * (nz - 1) : 0u - sxy, oz_hi = z + 1 == (int)nz ? sxy * (1u - nz) : sxy;
   const flag_t fl = a.flags[node];
   R f[M::Q];
+  using T = typename St::T;
+  if constexpr (A::per_plane) {
 #pragma unroll
-  for (int i = 0; i < M::Q; i++) {
-    const int o = (M::ex(i) > 0 ? ox_lo : (M::ex(i) < 0 ? ox_hi : 0)) +
-                  (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0)) +
-                  (M::DIM == 2 ? 0 : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0)));
-    f[i] = St::template load<R>(src + i * stride + o, R(M::w(i)));
+    for (int i = 0; i < M::Q; i++) {
+      const unsigned o = (M::ex(i) > 0 ? ox_lo : (M::ex(i) < 0 ? ox_hi : 0u)) +
+                         (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0u)) +
+                         (M::DIM == 2 ? 0u : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0u)));
+      f[i] = St::template load<R>(P.src(i) + (node + o), R(M::w(i)));
+    }
+    M::template run<R, G>(f, fl, a, g);
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) St::template store<R>(P.dst(i) + node, f[i], R(M::w(i)));
+  } else {
+    // one pointer at the node, planes reached by adding the stride
+    const T* __restrict__ src = P.s + node;
+    T* __restrict__ dst = P.d + node;
+    const size_t stride = P.stride;
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const int o = (int)((M::ex(i) > 0 ? ox_lo : (M::ex(i) < 0 ? ox_hi : 0u)) +
+                          (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0u)) +
+                          (M::DIM == 2 ? 0u : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0u))));
+      f[i] = St::template load<R>(src + i * stride + o, R(M::w(i)));
+    }
+    M::template run<R, G>(f, fl, a, g);
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) St::template store<R>(dst + i * stride, f[i], R(M::w(i)));
   }
-  M::template run<R, G>(f, fl, a, g);
-#pragma unroll
-  for (int i = 0; i < M::Q; i++) St::template store<R>(dst + i * stride, f[i], R(M::w(i)));
 }
 
 // Two nodes per thread for 16-bit storage: (x, x+1) with x even, so every
@@ -873,68 +979,90 @@ struct Pack16<StoreBF16<SH>> {
 };
 
 template <class M, class R, class St, bool G>
-__device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a, int x, int y, int z, int lane, R* g) {
-  using P = Pack16<St>;
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int sxy = nx * ny;
-  const int node = x + nx * y + sxy * z;  // even
-  const int oy_lo = y == 0 ? nx * (ny - 1) : -nx, oy_hi = y + 1 == ny ? nx * (1 - ny) : nx;
-  const int oz_lo = z == 0 ? sxy * (nz - 1) : -sxy, oz_hi = z + 1 == nz ? sxy * (1 - nz) : sxy;
-  const int o_prev = x == 0 ? nx - 2 : -2;       // pair (x-2, x-1), wrapped
-  const int o_next = x + 2 == nx ? 2 - nx : 2;   // pair (x+2, x+3), wrapped
-  const unsigned short* __restrict__ src = static_cast<const unsigned short*>(a.src) + node;
-  unsigned short* __restrict__ dst = static_cast<unsigned short*>(a.dst) + node;
-  const size_t stride = a.stride;
+__device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a,
+                                                 const PlaneAddr<typename St::T, M::Q>& P, int x, int y, int z,
+                                                 int lane, R* g) {
+  using P16 = Pack16<St>;
+  const unsigned nx = a.nx, ny = a.ny, nz = a.nz;
+  const unsigned sxy = nx * ny;
+  const unsigned node = x + nx * y + sxy * z;  // even
+  const unsigned oy_lo = y == 0 ? nx * (ny - 1) : 0u - nx, oy_hi = y + 1 == (int)ny ? nx * (1u - ny) : nx;
+  const unsigned oz_lo = z == 0 ? sxy * (nz - 1) : 0u - sxy, oz_hi = z + 1 == (int)nz ? sxy * (1u - nz) : sxy;
+  const unsigned o_prev = x == 0 ? nx - 2 : 0u - 2u;       // pair (x-2, x-1), wrapped
+  const unsigned o_next = x + 2 == (int)nx ? 2u - nx : 2u;  // pair (x+2, x+3), wrapped
   const unsigned fl2 = __ldg(reinterpret_cast<const unsigned*>(a.flags + node));
-  R fa[M::Q], fb[M::Q];
+  const flag_t fla = (flag_t)(fl2 & 0xffffu), flb = (flag_t)(fl2 >> 16);
+  float2 v[M::Q];  // (node x, node x+1)
 #pragma unroll
   for (int i = 0; i < M::Q; i++) {
-    const int o = (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0)) +
-                  (M::DIM == 2 ? 0 : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0)));
-    const unsigned short* p = src + i * stride + o;
-    const unsigned w = __ldg(reinterpret_cast<const unsigned*>(p));
-    const R sh = St::shifted ? R(M::w(i)) : R(0);
+    const unsigned o = (M::ey(i) > 0 ? oy_lo : (M::ey(i) < 0 ? oy_hi : 0u)) +
+                       (M::DIM == 2 ? 0u : (M::ez(i) > 0 ? oz_lo : (M::ez(i) < 0 ? oz_hi : 0u)));
+    const unsigned short* base = reinterpret_cast<const unsigned short*>(P.src(i));
+    const unsigned idx = node + o;
+    const unsigned w = __ldg(reinterpret_cast<const unsigned*>(base + idx));
     if (M::ex(i) == 0) {
-      const float2 v = P::unpack(w);
-      fa[i] = R(v.x) + sh;
-      fb[i] = R(v.y) + sh;
+      v[i] = P16::unpack(w);
     } else if (M::ex(i) > 0) {  // from x-1: (prev.hi, w.lo)
       unsigned prev = __shfl_up_sync(0xffffffffu, w, 1);
-      if (lane == 0) prev = __ldg(reinterpret_cast<const unsigned*>(p + o_prev));
-      fa[i] = R(P::hi(prev)) + sh;
-      fb[i] = R(P::lo(w)) + sh;
+      if (lane == 0) prev = __ldg(reinterpret_cast<const unsigned*>(base + (idx + o_prev)));
+      v[i] = make_float2(P16::hi(prev), P16::lo(w));
     } else {  // from x+1: (w.hi, next.lo)
       unsigned next = __shfl_down_sync(0xffffffffu, w, 1);
-      if (lane == 31) next = __ldg(reinterpret_cast<const unsigned*>(p + o_next));
-      fa[i] = R(P::hi(w)) + sh;
-      fb[i] = R(P::lo(next)) + sh;
+      if (lane == 31) next = __ldg(reinterpret_cast<const unsigned*>(base + (idx + o_next)));
+      v[i] = make_float2(P16::hi(w), P16::lo(next));
     }
   }
-  M::template run<R, G>(fa, (flag_t)(fl2 & 0xffffu), a, g);
-  M::template run<R, G>(fb, (flag_t)(fl2 >> 16), a, g);
+  bool packed = false;
+  if constexpr (!G && M::has_bulk && sizeof(R) == 4) {
+    // both nodes in the bulk: one packed FP32x2 collision for the pair
+    if (M::bulk(fla) && M::bulk(flb)) {
+      F2 f2[M::Q];
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
+      M::collide_bulk(f2, a);
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
+      packed = true;
+    }
+  }
+  if (!packed) {
+    R fa[M::Q], fb[M::Q];
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const R sh = St::shifted ? R(M::w(i)) : R(0);
+      fa[i] = R(v[i].x) + sh;
+      fb[i] = R(v[i].y) + sh;
+    }
+    M::template run<R, G>(fa, fla, a, g);
+    M::template run<R, G>(fb, flb, a, g);
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const R sh = St::shifted ? R(M::w(i)) : R(0);
+      v[i] = make_float2((float)(fa[i] - sh), (float)(fb[i] - sh));
+    }
+  }
 #pragma unroll
   for (int i = 0; i < M::Q; i++) {
-    const R sh = St::shifted ? R(M::w(i)) : R(0);
-    __stcs(reinterpret_cast<unsigned*>(dst + i * stride), P::pack((float)(fa[i] - sh), (float)(fb[i] - sh)));
+    unsigned short* base = reinterpret_cast<unsigned short*>(P.dst(i));
+    __stcs(reinterpret_cast<unsigned*>(base + node), P16::pack(v[i].x, v[i].y));
   }
 }
 
-// Block (32, by): each warp covers 64 consecutive x of one row.
-template <class M, class R, class St, bool G>
-__global__ void __launch_bounds__(256) k_iterate_pair(const Args<R, M::NSET> a) {
+// Block (32, M::PAIR_THREADS / 32): each warp covers 64 consecutive x of one
+// row. Plain iterations only (Globals iterations use k_iterate).
+template <class M, class R, class St>
+__global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
+    k_iterate_pair(const Args<R, M::NSET> a, const PlaneAddr<typename St::T, M::Q> P) {
   const int lane = threadIdx.x;
   const int x = 2 * (blockIdx.x * 32 + lane);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
-  R g[G ? M::NG : 1];
-#pragma unroll
-  for (int i = 0; i < (G ? M::NG : 1); i++) g[i] = 0;
-  if (y < a.ny) node_update_pair<M, R, St, G>(a, x, y, z, lane, g);  // y is uniform per warp
-  if constexpr (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+  R g[1];
+  if (y < a.ny) node_update_pair<M, R, St, false>(a, P, x, y, z, lane, g);  // y is uniform per warp
 }
 
-template <class M, class R, class St, bool G>
-__global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a) {
+template <class M, class R, class St, bool G, class A>
+__global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a, const A P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
@@ -942,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a) {
   R g[G ? M::NG : 1];
 #pragma unroll
   for (int i = 0; i < (G ? M::NG : 1); i++) g[i] = 0;
-  if (act) node_update<M, R, St, G>(a, x, y, z, g);
+  if (act) node_update<M, R, St, G>(a, P, x, y, z, g);
   if constexpr (G) reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
 }
 

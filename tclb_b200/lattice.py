@@ -271,5 +271,5 @@ class Lattice:
     def sync(self):
         _check(self.lib.tclb_sync(self._h))
 
-    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = False):
+    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True):
         _check(self.lib.tclb_set_launch(self._h, int(bx), int(by), (1 if use_graphs else 0) | (2 if use_pairs else 0)))
