@@ -173,10 +173,19 @@ int tclb_sync(tclb_h h);
    CUDA graph (on by default); TCLB_LAUNCH_PAIRS lets 16-bit storage with
    nx % 64 == 0 update two nodes per thread on plain iterations: 32-bit
    accesses, and for d3q19 / d3q27_cumulant bulk nodes one packed FP32x2
-   collision for both (on by default). bx, by shape the one-node kernel. */
+   collision for both (on by default); TCLB_LAUNCH_TMA lets 16-bit storage
+   with nx a multiple of 64 up to 256 (and ny a multiple of 512/nx) stage
+   tiles of whole rows in shared memory with TMA on plain iterations (on by
+   default; it takes precedence over PAIRS). bx, by shape the one-node kernel.
+   A staging wait that runs out (about a second) is reported as TCLB_ERR_CUDA
+   by the next tclb_sync or Globals-reading tclb_iterate. */
 #define TCLB_LAUNCH_GRAPHS 1
 #define TCLB_LAUNCH_PAIRS 2
+#define TCLB_LAUNCH_TMA 4
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);
+/* The launch shape and the paths plain iterations take on this lattice: the
+   flags that are both enabled and applicable (no TCLB counterpart). */
+int tclb_get_launch(tclb_h h, int* bx, int* by, int* flags);
 
 /* ---------------------------------------------------------------------------
    XML case files (<CLBConfig>): the control flow of TCLB's main and handler

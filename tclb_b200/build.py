@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtclb_b200.so")
 SOURCES = ["tclb_b200.cu", "batch.cu", "case.cpp"]
-HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "tclb_models.h", "cumulant_gen.cuh", "xml.hpp"]
+HEADERS = ["lbm_kernels.cuh", "lbm_batch.cuh", "lbm_tma.cuh", "f32x2.cuh", "tclb_models.h", "cumulant_gen.cuh", "xml.hpp"]
 RUNNER = os.path.join(HERE, "tclb_run")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -978,10 +978,56 @@ struct Pack16<StoreBF16<SH>> {
   }
 };
 
-template <class M, class R, class St, bool G>
+// Update and store two neighbouring nodes (x, x+1) of one row whose pulled
+// densities, as stored (shift not yet added), are v[i] = (node x, node x+1):
+// one packed FP32x2 collision when both are bulk nodes, else the scalar
+// node update twice. Plain iterations (no Globals).
+template <class M, class R, class St>
+__device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb,
+                                                  const Args<R, M::NSET>& a,
+                                                  const PlaneAddr<typename St::T, M::Q>& P, unsigned node) {
+  using P16 = Pack16<St>;
+  bool packed = false;
+  if constexpr (M::has_bulk && sizeof(R) == 4) {
+    // both nodes in the bulk: one packed FP32x2 collision for the pair
+    if (M::bulk(fla) && M::bulk(flb)) {
+      F2 f2[M::Q];
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
+      M::collide_bulk(f2, a);
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
+      packed = true;
+    }
+  }
+  if (!packed) {
+    R fa[M::Q], fb[M::Q];
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const R sh = St::shifted ? R(M::w(i)) : R(0);
+      fa[i] = R(v[i].x) + sh;
+      fb[i] = R(v[i].y) + sh;
+    }
+    R g[1];
+    M::template run<R, false>(fa, fla, a, g);
+    M::template run<R, false>(fb, flb, a, g);
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const R sh = St::shifted ? R(M::w(i)) : R(0);
+      v[i] = make_float2((float)(fa[i] - sh), (float)(fb[i] - sh));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < M::Q; i++) {
+    unsigned short* base = reinterpret_cast<unsigned short*>(P.dst(i));
+    __stcs(reinterpret_cast<unsigned*>(base + node), P16::pack(v[i].x, v[i].y));
+  }
+}
+
+template <class M, class R, class St>
 __device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a,
                                                  const PlaneAddr<typename St::T, M::Q>& P, int x, int y, int z,
-                                                 int lane, R* g) {
+                                                 int lane) {
   using P16 = Pack16<St>;
   const unsigned nx = a.nx, ny = a.ny, nz = a.nz;
   const unsigned sxy = nx * ny;
@@ -1012,40 +1058,7 @@ __device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a,
       v[i] = make_float2(P16::hi(w), P16::lo(next));
     }
   }
-  bool packed = false;
-  if constexpr (!G && M::has_bulk && sizeof(R) == 4) {
-    // both nodes in the bulk: one packed FP32x2 collision for the pair
-    if (M::bulk(fla) && M::bulk(flb)) {
-      F2 f2[M::Q];
-#pragma unroll
-      for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
-      M::collide_bulk(f2, a);
-#pragma unroll
-      for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
-      packed = true;
-    }
-  }
-  if (!packed) {
-    R fa[M::Q], fb[M::Q];
-#pragma unroll
-    for (int i = 0; i < M::Q; i++) {
-      const R sh = St::shifted ? R(M::w(i)) : R(0);
-      fa[i] = R(v[i].x) + sh;
-      fb[i] = R(v[i].y) + sh;
-    }
-    M::template run<R, G>(fa, fla, a, g);
-    M::template run<R, G>(fb, flb, a, g);
-#pragma unroll
-    for (int i = 0; i < M::Q; i++) {
-      const R sh = St::shifted ? R(M::w(i)) : R(0);
-      v[i] = make_float2((float)(fa[i] - sh), (float)(fb[i] - sh));
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < M::Q; i++) {
-    unsigned short* base = reinterpret_cast<unsigned short*>(P.dst(i));
-    __stcs(reinterpret_cast<unsigned*>(base + node), P16::pack(v[i].x, v[i].y));
-  }
+  pair_update_store<M, R, St>(v, fla, flb, a, P, node);
 }
 
 // Block (32, M::PAIR_THREADS / 32): each warp covers 64 consecutive x of one
@@ -1057,8 +1070,7 @@ __global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
   const int x = 2 * (blockIdx.x * 32 + lane);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
-  R g[1];
-  if (y < a.ny) node_update_pair<M, R, St, false>(a, P, x, y, z, lane, g);  // y is uniform per warp
+  if (y < a.ny) node_update_pair<M, R, St>(a, P, x, y, z, lane);  // y is uniform per warp
 }
 
 template <class M, class R, class St, bool G, class A>

@@ -1,0 +1,218 @@
+// Tile-staged iteration for 16-bit storage: a persistent kernel whose tiles
+// (R whole rows of one z plane) are copied into shared memory by TMA through
+// an S-stage mbarrier pipeline, then updated two nodes per thread.
+//
+// Why: with 16-bit densities the one-node and register-pair kernels are
+// limited by issue slots and by how many loads their registers can keep in
+// flight. Here the tensor-memory accelerator moves every population row of
+// the next S-1 tiles while the threads compute the current one, so memory
+// latency is hidden by the pipeline rather than by warps, and a pulled value
+// is one shared-memory load.
+//
+// Layout of a stage: Q population blocks then one flag block, each R rows of
+// nx 16-bit values (row-major, x fastest). For population i the block holds
+// the rows the tile pulls from: source row (y - e_y) mod ny of plane
+// (z - e_z) mod nz. A whole row is resident, so the x wrap is an index
+// modulo nx. Rows that do not wrap come as one R-row box; at the y faces the
+// rows come one by one (a second tensor map with a one-row box).
+//
+// Pipeline: a producer warp fills stage s (full[s] counts the bytes in);
+// eight consumer warps wait on full[s], read their values, release the stage
+// (one arrival each on empty[s]) and then compute, so copies of the next
+// tiles overlap the arithmetic. No block-wide barrier after set-up.
+//
+// Failure: every wait on an mbarrier is bounded (about a second of clock).
+// A warp whose wait runs out records an error code for the host and returns;
+// the other warps' waits then run out in turn, so the kernel always ends.
+#pragma once
+#include <cuda.h>
+
+#include "lbm_kernels.cuh"
+
+namespace tclb {
+
+struct TmaMaps {
+  CUtensorMap rows;  // densities of the source snapshot: dims (nx, ny, nz, Q), box (nx, R, 1, 1)
+  CUtensorMap row1;  // same tensor, box (nx, 1, 1, 1)
+  CUtensorMap flags;  // node types: dims (nx, ny, nz), box (nx, R, 1)
+};
+
+constexpr int TMA_STAGES = 3;
+constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
+constexpr int TMA_ERR_TIMEOUT = 1;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > TMA_WAIT_CYCLES) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Issue the copies of tile t into one stage; called by the whole producer
+// warp after lane 0 has armed the stage's full barrier. Lane i < Q copies
+// population i, lane Q the node types.
+template <class M>
+__device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage, unsigned bar, int t, int nx,
+                                         int ny, int nz, int R, int lane) {
+  const int rows_per_plane = ny / R;
+  const int z = t / rows_per_plane, y0 = (t % rows_per_plane) * R;
+  const unsigned block = (unsigned)R * nx;  // values per population block
+  if (lane < M::Q) {
+    const int i = lane;
+    const int ey = M::ey(i), ez = M::DIM == 2 ? 0 : M::ez(i);
+    int zs = z - ez;
+    zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
+    const unsigned dst = smem_u32(stage + (size_t)i * block);
+    const int ys = y0 - ey;
+    if (ys >= 0 && ys + R <= ny) {
+      tma_load_4d(dst, &T.rows, 0, ys, zs, i, bar);
+    } else {  // rows wrap at a y face: one row at a time
+      for (int r = 0; r < R; r++) {
+        int y = ys + r;
+        y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
+        tma_load_4d(dst + (unsigned)(r * nx * 2), &T.row1, 0, y, zs, i, bar);
+      }
+    }
+  } else if (lane == M::Q) {
+    tma_load_3d(smem_u32(stage + (size_t)M::Q * block), &T.flags, 0, y0, z, bar);
+  }
+}
+
+// The kernel: TMA_CONSUMERS warps update node pairs, one more warp (the last)
+// produces. Block = (TMA_CONSUMERS + 1) * 32 threads; the consumer warps
+// cover R*nx/2 pairs, one pair per thread per tile. Grid = resident blocks
+// (persistent), walking tiles t = blockIdx.x + k*gridDim.x.
+// Dynamic shared memory: 128 bytes of mbarriers (full[S], empty[S]), then
+// TMA_STAGES stages.
+constexpr int TMA_CONSUMERS = 8;
+constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
+
+template <class M, class R, class St>
+__global__ void __launch_bounds__(TMA_THREADS, 2)
+    k_iterate_tma(const Args<R, M::NSET> a, const __grid_constant__ TmaMaps T,
+                  const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err) {
+  static_assert(M::Q < 32, "one producer lane per population plus one for the node types");
+  using P16 = Pack16<St>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);
+  unsigned long long* empty = full + TMA_STAGES;
+  unsigned short* stages = reinterpret_cast<unsigned short*>(smem + 128);
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const unsigned block = (unsigned)R_rows * nx;
+  const size_t stage_elems = (size_t)(M::Q + 1) * block;
+  const int ntiles = nz * (ny / R_rows);
+  const int rows_per_plane = ny / R_rows;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    for (int s = 0; s < TMA_STAGES; s++) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), TMA_CONSUMERS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();  // the only block-wide barrier
+
+  if (warp == TMA_CONSUMERS) {  // producer
+    for (int k = 0;; k++) {
+      const int t = blockIdx.x + k * gridDim.x;
+      if (t >= ntiles) break;
+      const int s = k % TMA_STAGES;
+      const unsigned fb = smem_u32(&full[s]);
+      bool ok = true;
+      if (lane == 0 && k >= TMA_STAGES) ok = mbar_wait(smem_u32(&empty[s]), (unsigned)(k / TMA_STAGES - 1) & 1u);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
+        return;
+      }
+      if (lane == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * block * 2u);
+      }
+      __syncwarp();
+      tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);
+    }
+    return;
+  }
+
+  // consumers
+  const int half = nx >> 1;
+  const int r = tid / half, x = 2 * (tid % half);  // whole warps per row (nx >= 64)
+  const int xm = x == 0 ? nx - 1 : x - 1, xp2 = x + 2 == nx ? 0 : x + 2;
+  for (int k = 0;; k++) {
+    const int t = blockIdx.x + k * gridDim.x;
+    if (t >= ntiles) break;
+    const int s = k % TMA_STAGES;
+    const bool ok = mbar_wait(smem_u32(&full[s]), (unsigned)(k / TMA_STAGES) & 1u);
+    if (!__all_sync(0xffffffffu, ok)) {  // the warp leaves together
+      if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
+      return;
+    }
+    const unsigned short* st = stages + s * stage_elems;
+    const int z = t / rows_per_plane, y = (t % rows_per_plane) * R_rows + r;
+    float2 v[M::Q];
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) {
+      const unsigned short* row = st + (size_t)i * block + r * nx;
+      if (M::ex(i) == 0) {
+        v[i] = P16::unpack(*reinterpret_cast<const unsigned*>(row + x));
+      } else if (M::ex(i) > 0) {  // from x-1
+        v[i] = make_float2(P16::lo(row[xm]), P16::lo(row[x]));
+      } else {  // from x+1
+        v[i] = make_float2(P16::lo(row[x + 1]), P16::lo(row[xp2]));
+      }
+    }
+    const unsigned fl2 = *reinterpret_cast<const unsigned*>(st + (size_t)M::Q * block + r * nx + x);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(&empty[s]));  // this warp is done with the stage
+    const unsigned node = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)ny * (unsigned)z);
+    pair_update_store<M, R, St>(v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
+  }
+}
+
+}  // namespace tclb

@@ -8,6 +8,7 @@
 // independent and any number of lattices can share a GPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -17,7 +18,7 @@
 #include <vector>
 
 #include "../../include/tclb_b200.h"
-#include "lbm_kernels.cuh"
+#include "lbm_tma.cuh"
 
 using namespace tclb;
 
@@ -157,6 +158,11 @@ struct tclb_lattice {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int use_graphs = 1;
   int use_pairs = 1;  // 16-bit storage: two nodes per thread when nx % 64 == 0
+  // 16-bit storage: tile-staged TMA kernel (tma_rows rows per tile; tma[b]
+  // describes snapshot b as the source), and its error word in the pool
+  int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_grid = 0;
+  TmaMaps tma[2];
+  int* err_dev = nullptr;
 };
 
 struct Impl {
@@ -167,6 +173,7 @@ struct Impl {
   void (*color)(tclb_lattice*, int, void*, cudaStream_t);
   void (*to_double)(const void*, size_t, size_t, size_t, int, double*);   // storage -> double SoA
   void (*from_double)(const double*, size_t, size_t, size_t, int, void*);  // double SoA -> storage
+  void (*prepare)(tclb_lattice*);
   size_t real_size;
 };
 
@@ -210,6 +217,14 @@ struct Launch {
         P.s[i] = static_cast<const T*>(src) + (size_t)i * L->stride;
         P.d[i] = static_cast<T*>(dst) + (size_t)i * L->stride;
       }
+      if (L->use_tma && L->tma_ok && !glob) {  // tiles staged in shared memory by TMA
+        const int rows = L->tma_rows, threads = TMA_THREADS;
+        const size_t smem = 128 + (size_t)TMA_STAGES * (M::Q + 1) * rows * L->nx * sizeof(T);
+        if (L->tma_grid > 0) {
+          k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev);
+          return;
+        }
+      }
       if (L->use_pairs && !glob && L->nx % 64 == 0) {  // two nodes per thread, 32-bit accesses
         constexpr int by = M::PAIR_THREADS / 32;
         const dim3 blk(32, by), grd(L->nx / 64, (L->ny + by - 1) / by, L->nz);
@@ -222,6 +237,27 @@ struct Launch {
       const StrideAddr<T> P{static_cast<const T*>(src), static_cast<T*>(dst), L->stride};
       if (glob) k_iterate<M, R, St, true><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
       else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
+    }
+  }
+  // Once at creation: shared-memory opt-in and persistent grid of the
+  // tile-staged kernel (resident blocks per SM x SMs, at most one per tile).
+  static void prepare(tclb_lattice* L) {
+    using T = typename St::T;
+    if constexpr (sizeof(T) == 2) {
+      if (!L->tma_ok) return;
+      const int rows = L->tma_rows, threads = TMA_THREADS;
+      const size_t smem = 128 + (size_t)TMA_STAGES * (M::Q + 1) * rows * L->nx * sizeof(T);
+      int per_sm = 0, sms = 0;
+      if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+              cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_iterate_tma<M, R, St>, threads, smem) !=
+              cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, L->device) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        L->tma_ok = 0;
+        return;
+      }
+      L->tma_grid = std::min(L->nz * (L->ny / rows), per_sm * sms);
     }
   }
   static void init(tclb_lattice* L, cudaStream_t s) {
@@ -255,7 +291,8 @@ struct Launch {
       for (size_t n = 0; n < N; n++) p[(size_t)q * stride + n] = St::from_double(in[(size_t)q * N + n], M::w(q));
   }
   static const Impl* get() {
-    static const Impl impl = {iterate, init, quantity, equilibrium, color, to_double, from_double, sizeof(R)};
+    static const Impl impl = {iterate, init, quantity, equilibrium, color, to_double, from_double, prepare,
+                              sizeof(R)};
     return &impl;
   }
 };
@@ -283,6 +320,76 @@ const Impl* impl_for(int model, int precision, int storage) {
 }
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Tensor maps of the tile-staged kernel (16-bit storage, nx a multiple of 64
+// and at most 256, R = 512 / nx rows per tile dividing ny). The encoder is the
+// driver's cuTensorMapEncodeTiled, reached through the runtime's entry-point
+// query so the library links only the runtime. When anything does not fit,
+// tma_ok stays 0 and the register kernels run.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+void setup_tma(tclb_lattice* L) {
+  L->tma_ok = 0;
+  if (L->elem != 2 || L->nx % 64 || L->nx > 256) return;
+  const int R = 512 / L->nx;
+  if (L->ny % R) return;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return;
+  const cuuint64_t e = 2;
+  const cuuint64_t dims[4] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz, (cuuint64_t)L->T->Q};
+  const cuuint64_t strides[3] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e, L->stride * e};
+  const cuuint32_t box_rows[4] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1, 1};
+  const cuuint32_t box_row1[4] = {(cuuint32_t)L->nx, 1, 1, 1};
+  const cuuint32_t ones[4] = {1, 1, 1, 1};
+  for (int b = 0; b < 2; b++) {
+    if (enc(&L->tma[b].rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, L->buf[b], dims, strides, box_rows, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return;
+    if (enc(&L->tma[b].row1, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, L->buf[b], dims, strides, box_row1, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return;
+    const cuuint64_t fdims[3] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz};
+    const cuuint64_t fstrides[2] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e};
+    const cuuint32_t fbox[3] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1};
+    if (enc(&L->tma[b].flags, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, L->flags, fdims, fstrides, fbox, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return;
+  }
+  L->tma_rows = R;
+  L->tma_ok = 1;
+}
+
+// An mbarrier wait of the tile-staged kernel ran out: the iteration it was in
+// did not update every node.
+int check_device_error(tclb_lattice* L, cudaStream_t s) {
+  int e = 0;
+  TCLB_CK(cudaMemcpyAsync(&e, L->err_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  if (e == TMA_ERR_TIMEOUT) {
+    TCLB_CK(cudaMemsetAsync(L->err_dev, 0, sizeof(int), s));
+    return fail(TCLB_ERR_CUDA, "tile pipeline: a wait for staged tiles ran out; the state is not valid");
+  }
+  return TCLB_OK;
+}
 
 int upload_zone(tclb_lattice* L) {
   const size_t n = L->zone.size();
@@ -352,7 +459,7 @@ int calc_globals(tclb_lattice* L, cudaStream_t s) {
   TCLB_CK(cudaStreamSynchronize(s));
   for (size_t i = 0; i < tab.size(); i++) L->globals[i] += tab[i];
   TCLB_CK(cudaMemsetAsync(L->glob_dev, 0, tab.size() * sizeof(double), s));
-  return TCLB_OK;
+  return check_device_error(L, s);
 }
 
 #define CHECK_H(h) \
@@ -429,7 +536,7 @@ int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, i
   const size_t flagb = align_up(N * sizeof(flag_t), 256);
   const size_t zoneb = align_up((size_t)L->nzones * T->nzonesettings * impl->real_size, 256);
   const size_t globb = align_up(T->nglobals * sizeof(double), 256);
-  const size_t total = 2 * bufb + flagb + zoneb + globb;
+  const size_t total = 2 * bufb + flagb + zoneb + globb + 256;
   cudaError_t e = cudaMalloc((void**)&L->pool, total);
   if (e != cudaSuccess) {
     delete L;
@@ -441,6 +548,7 @@ int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, i
   L->flags = reinterpret_cast<flag_t*>(L->pool + 2 * bufb);
   L->zone_dev = L->pool + 2 * bufb + flagb;
   L->glob_dev = reinterpret_cast<double*>(L->pool + 2 * bufb + flagb + zoneb);
+  L->err_dev = reinterpret_cast<int*>(L->pool + 2 * bufb + flagb + zoneb + globb);
   e = cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaFree(L->pool);
@@ -467,6 +575,8 @@ int tclb_create(tclb_h* out, int model, int nx, int ny, int nz, int precision, i
     delete L;
     return rc;
   }
+  setup_tma(L);
+  impl->prepare(L);
   *out = L;
   return TCLB_OK;
 }
@@ -915,13 +1025,26 @@ int tclb_set_launch(tclb_h L, int bx, int by, int flags) {
   L->by = by;
   L->use_graphs = (flags & TCLB_LAUNCH_GRAPHS) ? 1 : 0;
   L->use_pairs = (flags & TCLB_LAUNCH_PAIRS) ? 1 : 0;
+  L->use_tma = (flags & TCLB_LAUNCH_TMA) ? 1 : 0;
+  return TCLB_OK;
+}
+
+int tclb_get_launch(tclb_h L, int* bx, int* by, int* flags) {
+  CHECK_H(L);
+  if (bx) *bx = L->bx;
+  if (by) *by = L->by;
+  if (flags) {
+    const bool tma = L->use_tma && L->tma_ok && L->tma_grid > 0;
+    const bool pairs = !tma && L->use_pairs && L->elem == 2 && L->nx % 64 == 0;
+    *flags = (L->use_graphs ? TCLB_LAUNCH_GRAPHS : 0) | (pairs ? TCLB_LAUNCH_PAIRS : 0) | (tma ? TCLB_LAUNCH_TMA : 0);
+  }
   return TCLB_OK;
 }
 
 int tclb_sync(tclb_h L) {
   CHECK_H(L);
   TCLB_CK(cudaStreamSynchronize(L->stream));
-  return TCLB_OK;
+  return check_device_error(L, L->stream);
 }
 
 }  // extern "C"

@@ -77,6 +77,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_save_pri.argtypes = [h, vp, sz]
     L.tclb_load_pri.argtypes = [h, vp, sz]
     L.tclb_color.argtypes = [h, vp, i, i, vp]
+    L.tclb_get_launch.argtypes = [h, ip, ip, ip]
     _lib = L
     return L
 
@@ -271,5 +272,13 @@ class Lattice:
     def sync(self):
         _check(self.lib.tclb_sync(self._h))
 
-    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True):
-        _check(self.lib.tclb_set_launch(self._h, int(bx), int(by), (1 if use_graphs else 0) | (2 if use_pairs else 0)))
+    def launch_path(self) -> dict:
+        """The paths plain iterations take: graphs, pairs, tma (enabled and applicable)."""
+        bx, by, fl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.tclb_get_launch(self._h, ctypes.byref(bx), ctypes.byref(by), ctypes.byref(fl)))
+        return {"bx": bx.value, "by": by.value, "graphs": bool(fl.value & 1), "pairs": bool(fl.value & 2),
+                "tma": bool(fl.value & 4)}
+
+    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True, use_tma: bool = True):
+        flags = (1 if use_graphs else 0) | (2 if use_pairs else 0) | (4 if use_tma else 0)
+        _check(self.lib.tclb_set_launch(self._h, int(bx), int(by), flags))

@@ -1,0 +1,106 @@
+"""16-bit storage paths of a plain iteration: the tile-staged kernel (whole rows
+copied into shared memory by TMA), the register two-node kernel and the
+one-node kernel.
+
+The tile-staged and register two-node kernels run the same update on the same
+pulled values (packed FP32x2 collision for bulk pairs, the scalar node update
+otherwise); only the route of the loads differs, so their snapshots must be
+identical bit for bit. The one-node kernel contracts its arithmetic
+differently, so it is compared within a rounding bar, and all three against
+the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from tclb_b200 import models as M
+from tclb_b200.lattice import Lattice
+
+from helpers import apply_params, perturbed_equilibrium, random_flags, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TYPES = {
+    "d2q9": ["Wall", "Solid", "WVelocity", "EPressure", "NSymmetry"],
+    "d3q19": ["Wall", "Solid", "WVelocity", "EPressure", "WPressure"],
+    "d3q27_cumulant": ["Wall", "Solid", "WVelocity", "EPressure", "NVelocity", "Buffer"],
+}
+PARAMS = {
+    "d2q9": [("setting", "Viscosity", 0.05), ("zone", "VelocityX", 0.02, 1), ("zone", "Pressure", 0.01, 2)],
+    "d3q19": [("setting", "nu", 0.05), ("setting", "InletVelocity", 0.02), ("setting", "ForceX", 1e-5)],
+    "d3q27_cumulant": [("setting", "nu", 0.02), ("setting", "nubuffer", 0.05), ("setting", "ForceX", 1e-5),
+                       ("zone", "Velocity", 0.02, 1), ("zone", "Pressure", 0.01, 2)],
+}
+# (nz, ny, nx): rows per tile = 512 / nx; ny a multiple of it. Small ny makes
+# most tiles wrap at a y face (the one-row copies), larger ny has inner tiles.
+SHAPES = {
+    "d2q9": [(1, 16, 128), (1, 8, 64), (1, 6, 256)],
+    "d3q19": [(4, 8, 64), (3, 12, 128), (3, 6, 256)],
+    "d3q27_cumulant": [(4, 8, 64), (3, 12, 128), (2, 6, 256)],
+}
+
+
+def run(model, shape, storage, fl, f0, tma, pairs, niter=5):
+    m = M.get(model)
+    g = Lattice(model, shape[2], shape[1], shape[0], precision="fp32", storage=storage)
+    g.set_launch(32, 8, use_graphs=True, use_pairs=pairs, use_tma=tma)
+    path = g.launch_path()
+    g.set_flags(fl)
+    apply_params(g, PARAMS[model])
+    g.set_densities(f0)
+    g.Iterate(niter, M.ITER_NORM | M.ITER_LASTGLOB)
+    g.sync()
+    out = (g.save().copy(), g.densities(), g.globals)
+    g.close()
+    return path, out
+
+
+@pytest.mark.parametrize("storage", ["fp16s", "bf16s"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_tile_staged_matches_register_pairs_bit_for_bit(model, storage):
+    m = M.get(model)
+    for k, shape in enumerate(SHAPES[model]):
+        extra = [g for g in ("ADDITIONALS", "BODY", "OBJECTIVE") if g in m.groups]
+        fl = random_flags(model, shape, [t for t in TYPES[model] if t in m.node_types], zones=3, seed=20 + k,
+                          p_type=0.15, extra_groups=extra[:1])
+        f0 = perturbed_equilibrium(model, shape, seed=30 + k)
+        p_tma, (raw_tma, f_tma, g_tma) = run(model, shape, storage, fl, f0, tma=True, pairs=True)
+        p_pair, (raw_pair, f_pair, g_pair) = run(model, shape, storage, fl, f0, tma=False, pairs=True)
+        p_one, (raw_one, f_one, g_one) = run(model, shape, storage, fl, f0, tma=False, pairs=False)
+        assert p_tma["tma"] and not p_pair["tma"] and p_pair["pairs"] and not (p_one["tma"] or p_one["pairs"])
+        assert np.isfinite(f_tma).all()
+        assert raw_tma.tobytes() == raw_pair.tobytes(), f"{shape}: tile-staged and register pairs differ"
+        assert np.allclose(g_tma, g_pair, rtol=1e-12, atol=1e-12)  # FP64 atomics: order may differ
+        assert rel_l2(f_tma, f_one) < 1e-3, shape
+        o = oracle.OracleLattice(model, shape[2], shape[1], shape[0], precision="fp64")
+        o.set_flags(fl)
+        apply_params(o, PARAMS[model])
+        o.set_densities(f0)
+        o.iterate(5, M.ITER_NORM | M.ITER_LASTGLOB)
+        ref = o.densities()
+        e_one, e_tma = rel_l2(f_one, ref), rel_l2(f_tma, ref)
+        assert e_tma < 1.5 * e_one + 1e-6, (shape, e_one, e_tma)
+
+
+def test_tile_staged_only_where_it_applies():
+    # FP32 storage, nx not a multiple of 64, nx above 256, ny not a multiple of 512/nx: no TMA
+    for args in [("d3q19", 64, 8, 2, "same"), ("d3q19", 96, 8, 2, "fp16s"), ("d3q19", 512, 4, 2, "fp16s"),
+                 ("d3q19", 128, 6, 2, "fp16s")]:
+        model, nx, ny, nz, st = args
+        g = Lattice(model, nx, ny, nz, precision="fp32", storage=st)
+        assert not g.launch_path()["tma"], args
+        g.close()
+    g = Lattice("d3q27_cumulant", 256, 4, 2, precision="fp32", storage="fp16s")
+    assert g.launch_path()["tma"]
+    g.close()
+
+
+def test_tile_staged_long_run_stays_identical():
+    """Many replays of the captured iteration graph (tiles refill every stage
+    many times) still match the register pair path."""
+    model, shape, storage = "d3q27_cumulant", (8, 16, 128), "fp16s"
+    m = M.get(model)
+    fl = np.full(shape, m.flag("MRT"), np.uint16)
+    f0 = perturbed_equilibrium(model, shape, seed=5)
+    _, (raw_tma, _, _) = run(model, shape, storage, fl, f0, tma=True, pairs=True, niter=130)
+    _, (raw_pair, _, _) = run(model, shape, storage, fl, f0, tma=False, pairs=True, niter=130)
+    assert raw_tma.tobytes() == raw_pair.tobytes()
