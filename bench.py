@@ -55,16 +55,18 @@ def parse():
     p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--pairs", type=int, default=1,
-                   help="0 = one node per thread also for 16-bit storage (default 1: two nodes per "
-                        "thread when nx is a multiple of 64)")
+    p.add_argument("--path", default="auto", choices=["auto", "tma", "pairs", "one"],
+                   help="16-bit storage kernel for plain iterations: auto (tile-staged TMA where it "
+                        "applies, else two nodes per thread), tma, pairs, one (one node per thread)")
     p.add_argument("--config", type=int, default=2,
                    help="2 = the headline Taylor-Green line; 1, 3, 4, 5 = the other configurations (one JSON line)")
     return p.parse_args()
 
 
 def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    from tclb_b200.replicas import env
+
+    return env()
 
 
 # ---------------------------------------------------------------------------
@@ -231,28 +233,13 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
+    from tclb_b200.replicas import Replicas
+
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            t = torch.ones(1, device="cuda")
-            dist.all_reduce(t)
-        torch.cuda.synchronize()
-
-    def reduce_max(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    # replicas only: one lattice per GPU, host coordination over NCCL
+    reps = Replicas("nccl")
+    barrier, reduce_max = reps.barrier, reps.reduce_max
 
     from tclb_b200 import models as M
     from tclb_b200.lattice import Lattice
@@ -264,8 +251,10 @@ def run_ours(args):
         cpu = cpu_baseline(args, args.model, args.cpu_seconds)
 
     lat = Lattice(args.model, n, n, n, precision=args.precision, storage=args.storage)
-    if not args.pairs:
-        lat.set_launch(128 if n >= 128 else 32, 2 if n >= 128 else 8, use_graphs=True, use_pairs=False)
+    if args.path != "auto":
+        lat.set_launch(128 if n >= 128 else 32, 2 if n >= 128 else 8, use_graphs=True,
+                       use_pairs=args.path in ("pairs", "tma"), use_tma=args.path == "tma")
+    path = lat.launch_path()
     tgv_setup(lat, n)
     # a dedicated (non-default) stream: the library launches on it, the CUDA
     # events below are recorded on it
@@ -303,12 +292,11 @@ def run_ours(args):
     wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
     t = e_start.elapsed_time(e_end) / 1e3
-    t_max = reduce_max(t)
     kern = sum(a.elapsed_time(b) for a, b in pairs) / 1e3 / (args.steps * (I - 1))
     kern = reduce_max(kern)
     glob = lat.globals_dict()
     updates = N * I * args.steps
-    value = updates * world / t_max / 1e6
+    value, t_max = reps.whole_job_rate(updates / 1e6, t)
 
     peaks, peak_src = measured_peaks()
     achieved = bpu * N / kern / 1e9
@@ -355,14 +343,13 @@ def run_ours(args):
                            "model": args.model, "lattice": [n, n, n], "precision": args.precision,
                            "storage": args.storage, "iterations_per_step": I, "globals_every": I,
                            "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % (bpu / 2 * N / 1e9),
-                           "parallelism": f"replicas x{world}", "two_nodes_per_thread": bool(args.pairs) and args.storage != "same" and n % 64 == 0},
+                           "parallelism": f"replicas x{world}", "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": args.steps * I, "wall_s": wall,
                 "globals_last": {k: float(v) for k, v in glob.items()}}
         print(json.dumps(line), flush=True)
     lat.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 

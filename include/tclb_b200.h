@@ -174,9 +174,9 @@ int tclb_sync(tclb_h h);
    nx % 64 == 0 update two nodes per thread on plain iterations: 32-bit
    accesses, and for d3q19 / d3q27_cumulant bulk nodes one packed FP32x2
    collision for both (on by default); TCLB_LAUNCH_TMA lets 16-bit storage
-   with nx a multiple of 64 up to 256 (and ny a multiple of 512/nx) stage
-   tiles of whole rows in shared memory with TMA on plain iterations (on by
-   default; it takes precedence over PAIRS). bx, by shape the one-node kernel.
+   stage tiles of whole rows in shared memory with TMA on plain iterations
+   (on by default; it takes precedence over PAIRS) when nx is a multiple of 64
+   up to 256 with ny a multiple of 512/nx, or nx is 384 or 512. bx, by shape the one-node kernel.
    A staging wait that runs out (about a second) is reported as TCLB_ERR_CUDA
    by the next tclb_sync or Globals-reading tclb_iterate. */
 #define TCLB_LAUNCH_GRAPHS 1
