@@ -2,14 +2,15 @@
 """Benchmark of the lattice-Boltzmann hot path on B200.
 
 Workload (N=1 line): d3q27_cumulant, FP32, triply periodic Taylor-Green vortex
-on 256^3 nodes (u0=0.05, rho0=1, nu=1e-3), Globals every 50 iterations -- the
-configuration the MLUPS metric is quoted on. A *step* is one logging interval:
-49 plain iterations plus one iteration that integrates the Globals
-(ITER_LASTGLOB) and reads them back. ``value`` is MLUPS over K steps with the
-lattice resident in HBM; ``e2e`` is the same metric through the C ABI from
+on 256^3 nodes (u0=0.05, rho0=1, nu=1e-3), Globals, kinetic energy and
+enstrophy every 50 iterations -- the configuration the MLUPS metric is quoted
+on. A *step* is one logging interval: 49 plain iterations, one iteration that
+integrates the Globals (ITER_LASTGLOB) and reads them back, and the kinetic
+energy / enstrophy reduction read back. ``value`` is MLUPS over K steps with
+the lattice resident in HBM; ``e2e`` is the same metric through the C ABI from
 host buffers: each e2e step uploads the initial snapshot from pinned host
-memory, runs the full 2000-iteration case with Globals every 50, and reads the
-velocity field back.
+memory, runs the full 2000-iteration case with the same diagnostics every 50,
+and reads the velocity field back.
 
 Multi-GPU (torchrun, one rank per GPU): independent replicas, weak scaling, no
 data-path collective (the case does not shard across GPUs here).
@@ -285,6 +286,7 @@ def run_ours(args):
         lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
         b.record(stream)
         lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        energy = lat.energy_enstrophy(stream=sp)  # kinetic energy and enstrophy every I iterations
         pairs.append((a, b))
     e_end.record(stream)
     torch.cuda.synchronize()
@@ -324,15 +326,17 @@ def run_ours(args):
             for _ in range(nlog):
                 lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
                 lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+                lat.energy_enstrophy(stream=sp)
             lat.GetQuantity("U", out=uview, stream=sp)
         s1.record(stream)
         torch.cuda.synchronize()
         te = reduce_max(s0.elapsed_time(s1) / 1e3)
         e2e = {"value": N * nlog * I * args.e2e_steps * world / te / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": int(snap.numel()),
-               "d2h_bytes_per_step": int(ubuf.numel() * ubuf.element_size() + nlog * gl_bytes),
+               "d2h_bytes_per_step": int(ubuf.numel() * ubuf.element_size() + nlog * (gl_bytes + 16)),
                "steps": args.e2e_steps, "iterations_per_step": nlog * I,
-               "step": "upload snapshot (pinned), full case with Globals every 50, read U back"}
+               "step": "upload snapshot (pinned), full case with Globals, kinetic energy and enstrophy every "
+                       "50 iterations, read U back"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -342,11 +346,13 @@ def run_ours(args):
                                        f"nu={TGV_NU[args.model]:g}",
                            "model": args.model, "lattice": [n, n, n], "precision": args.precision,
                            "storage": args.storage, "iterations_per_step": I, "globals_every": I,
+                           "energy_enstrophy_every": I,
                            "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % (bpu / 2 * N / 1e9),
                            "parallelism": f"replicas x{world}", "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-                "gpu_launches": args.steps * I, "wall_s": wall,
-                "globals_last": {k: float(v) for k, v in glob.items()}}
+                "gpu_launches": args.steps * (I + 2), "wall_s": wall,
+                "globals_last": dict({k: float(v) for k, v in glob.items()}, KineticEnergy=energy[0],
+                                     Enstrophy=energy[1])}
         print(json.dumps(line), flush=True)
     lat.close()
     reps.close()

@@ -124,6 +124,14 @@ int tclb_get_quantity(tclb_h h, int q, const int region[6], void* out, double sc
    returns after the copy). */
 int tclb_color(tclb_h h, void* rgba, int z, int on_host, void* stream);
 
+/* Flow diagnostics of the current snapshot (no TCLB counterpart: TCLB has no
+   such Globals, its users reduce an exported U field): out[0] = kinetic energy
+   1/2 sum |U|^2, out[1] = enstrophy 1/2 sum |curl U|^2, in lattice units, with
+   U the model's velocity quantity and the curl by second-order central
+   differences on the periodic lattice; FP64 sums over all nodes. Uses the
+   quantity staging buffer (allocated on first use); returns after the copy. */
+int tclb_energy_enstrophy(tclb_h h, double* out, void* stream);
+
 /* Same result as tclb_get_quantity, for callers that must not allocate device
    memory: an application whose GPU memory is all owned by its own pool or
    admission budget, or a latency-critical loop where cudaMalloc/cudaFree would
@@ -176,7 +184,7 @@ int tclb_sync(tclb_h h);
    collision for both (on by default); TCLB_LAUNCH_TMA lets 16-bit storage
    stage tiles of whole rows in shared memory with TMA on plain iterations
    (on by default; it takes precedence over PAIRS) when nx is a multiple of 64
-   up to 256 with ny a multiple of 512/nx, or nx is 384 or 512. bx, by shape the one-node kernel.
+   up to 256 and ny a multiple of 512/nx. bx, by shape the one-node kernel.
    A staging wait that runs out (about a second) is reported as TCLB_ERR_CUDA
    by the next tclb_sync or Globals-reading tclb_iterate. */
 #define TCLB_LAUNCH_GRAPHS 1

@@ -112,9 +112,12 @@ struct D2Q9 {
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
   static constexpr bool has_bulk = false;  // no packed two-node collision
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 1;
-  __device__ __forceinline__ static bool bulk(flag_t) { return false; }
-  template <class V, class R>
-  __device__ __forceinline__ static void collide_bulk(V (&)[Q], const Args<R, NSET>&) {}
+  __device__ __forceinline__ static bool collides(flag_t) { return false; }
+  __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
+  template <class R>
+  __device__ __forceinline__ static void pre_collision(R (&)[Q], flag_t, const Args<R, NSET>&) {}
+  template <class R>
+  __device__ __forceinline__ static void collide_pair(F2 (&)[Q], flag_t, flag_t, const Args<R, NSET>&) {}
   template <class R>
   __host__ __device__ static void derived(const R*, R* k) { k[0] = k[1] = k[2] = k[3] = R(0); }
   __host__ __device__ static constexpr int ex(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0); }
@@ -438,16 +441,6 @@ struct D3Q19 {
     }
   }
 
-  // A node with no boundary type and the MRT collision, without Globals.
-  __device__ __forceinline__ static bool bulk(flag_t fl) {
-    return (fl & d3q19::BOUNDARY) == 0 && (fl & d3q19::COLLISION) == d3q19::MRT;
-  }
-  template <class V, class R>
-  __device__ __forceinline__ static void collide_bulk(V (&f)[Q], const Args<R, NSET>& a) {
-    V rho, jx, jy, jz;
-    trt(f, a, rho, jx, jy, jz);
-  }
-
   template <class R, bool G>
   __device__ __forceinline__ static void mrt(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g, const R* zs) {
     R rho, jx, jy, jz;
@@ -477,6 +470,13 @@ struct D3Q19 {
   template <class R, bool G>
   __device__ __forceinline__ static void run(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g) {
     const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    boundaries(f, fl, a);
+    if ((fl & d3q19::COLLISION) == d3q19::MRT) mrt<R, G>(f, fl, a, g, zs);
+  }
+
+  // BOUNDARY group of Run (:181-204)
+  template <class R>
+  __device__ __forceinline__ static void boundaries(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
     const unsigned b = fl & d3q19::BOUNDARY;
     if (b) {
       switch (b) {  // :181-204
@@ -524,7 +524,21 @@ struct D3Q19 {
         default: break;
       }
     }
-    if ((fl & d3q19::COLLISION) == d3q19::MRT) mrt<R, G>(f, fl, a, g, zs);
+  }
+
+  // Two nodes with one packed collision: boundaries per node, then the
+  // two-rate update on both lanes (a lane whose node does not collide keeps
+  // its values; the rates are the same for every node).
+  __device__ __forceinline__ static bool collides(flag_t fl) { return (fl & d3q19::COLLISION) == d3q19::MRT; }
+  __device__ __forceinline__ static bool has_boundary(flag_t fl) { return (fl & d3q19::BOUNDARY) != 0; }
+  template <class R>
+  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
+    boundaries(f, fl, a);
+  }
+  template <class R>
+  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const Args<R, NSET>& a) {
+    F2 rho, jx, jy, jz;
+    trt(f, a, rho, jx, jy, jz);
   }
 
   // SetEquilibrum (:212-217): f = Req(rho, J) . MRTMAT.inv
@@ -738,16 +752,26 @@ struct D3Q27C {
     for (int r = 0; r < 9; r++) unraw3(f[r], f[r + 9], f[r + 18]);
   }
 
-  // A node with no boundary type or extra group and the MRT collision,
-  // without Globals; V = R, or F2 for two nodes.
-  __device__ __forceinline__ static bool bulk(flag_t fl) {
-    return (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) == 0 && (fl & d3q27c::COLLISION) == d3q27c::MRT;
+  // Two nodes with one packed collision: boundaries per node (no Globals),
+  // then the cumulant collision on both lanes with each node's rate (nubuffer
+  // on BOUNDARY nodes); a lane whose node does not collide keeps its values.
+  __device__ __forceinline__ static bool collides(flag_t fl) { return (fl & d3q27c::COLLISION) == d3q27c::MRT; }
+  __device__ __forceinline__ static bool has_boundary(flag_t fl) {
+    return (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) != 0;
   }
-  template <class V, class R>
-  __device__ __forceinline__ static void collide_bulk(V (&f)[Q], const Args<R, NSET>& a) {
+  template <class R>
+  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
+    if (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) {
+      R g[1];
+      boundaries<R, false>(f, fl, g, a.zone + (fl >> ZONE_SHIFT) * NZS);
+    }
+  }
+  template <class R>
+  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t fla, flag_t flb, const Args<R, NSET>& a) {
+    const F2 w0((float)((fla & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]), (float)((flb & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]));
     to_raw(f);
-    if (a.s[d3q27c::S_Omega] == R(1)) relax<V, R, false>(f, a, V(a.k[0]));
-    else relax<V, R, true>(f, a, V(a.k[0]));
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<F2, R, false>(f, a, w0);
+    else relax<F2, R, true>(f, a, w0);
     from_raw(f);
   }
 
@@ -979,28 +1003,63 @@ struct Pack16<StoreBF16<SH>> {
 };
 
 // Update and store two neighbouring nodes (x, x+1) of one row whose pulled
-// densities, as stored (shift not yet added), are v[i] = (node x, node x+1):
-// one packed FP32x2 collision when both are bulk nodes, else the scalar
-// node update twice. Plain iterations (no Globals).
+// densities, as stored (shift not yet added), are v[i] = (node x, node x+1).
+// Models with a packed collision: boundary conditions per node, then one
+// FP32x2 collision for both; others: the scalar node update twice. Plain
+// iterations (no Globals).
 template <class M, class R, class St>
 __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb,
                                                   const Args<R, M::NSET>& a,
                                                   const PlaneAddr<typename St::T, M::Q>& P, unsigned node) {
   using P16 = Pack16<St>;
-  bool packed = false;
   if constexpr (M::has_bulk && sizeof(R) == 4) {
-    // both nodes in the bulk: one packed FP32x2 collision for the pair
-    if (M::bulk(fla) && M::bulk(flb)) {
-      F2 f2[M::Q];
+    // Values stay packed (node x, node x+1). A node with a boundary type has
+    // its lane taken out, updated by the scalar boundary code and put back;
+    // then one packed FP32x2 collision serves both nodes, so bulk and
+    // boundary pairs do not diverge in the collision.
+    F2 f2[M::Q];
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
-      M::collide_bulk(f2, a);
+    for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
+    if (M::has_boundary(fla)) {
+      float t[M::Q];
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
-      packed = true;
+      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.x;
+      M::pre_collision(t, fla, a);
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) f2[i].v.x = t[i];
     }
-  }
-  if (!packed) {
+    if (M::has_boundary(flb)) {
+      float t[M::Q];
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.y;
+      M::pre_collision(t, flb, a);
+#pragma unroll
+      for (int i = 0; i < M::Q; i++) f2[i].v.y = t[i];
+    }
+    const bool ca = M::collides(fla), cb = M::collides(flb);
+    if (ca || cb) {
+      // A pair where only one node collides (fluid next to a wall) parks the
+      // other node's values in thread-local memory across the collision; a
+      // volatile array keeps them out of the registers every pair would pay.
+      float keep_mem[M::Q];
+      volatile float* keep = keep_mem;
+      const bool mixed = ca != cb;
+      if (mixed) {
+#pragma unroll
+        for (int i = 0; i < M::Q; i++) keep[i] = ca ? f2[i].v.y : f2[i].v.x;
+      }
+      M::collide_pair(f2, fla, flb, a);
+      if (mixed) {
+#pragma unroll
+        for (int i = 0; i < M::Q; i++) {
+          if (ca) f2[i].v.y = keep[i];
+          else f2[i].v.x = keep[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
+  } else {
     R fa[M::Q], fb[M::Q];
 #pragma unroll
     for (int i = 0; i < M::Q; i++) {
@@ -1217,6 +1276,52 @@ __global__ void k_color(const Args<R, M::NSET> a, int z, uchar4* out) {
   R u[3];
   M::template quantity<R>(1, f, fl, a, u);
   out[x + (size_t)nx * y] = color_map(speed<R>(u, M::DIM == 3), M::color_weight(fl));
+}
+
+// Kinetic energy and enstrophy of a velocity field (3 values per node, x
+// fastest): E = 1/2 sum |u|^2 and Omega = 1/2 sum |curl u|^2 with second-order
+// central differences on the periodic lattice (lattice units, dx = 1). FP64
+// per-thread values, block reduction in shared memory, one FP64 atomic per
+// block and quantity. 2D lattices (nz = 1) have only the z vorticity.
+template <class R>
+__global__ void __launch_bounds__(256) k_energy_enstrophy(const R* __restrict__ u, int nx, int ny, int nz,
+                                                          double* out) {
+  __shared__ double sh[2][256];
+  const int tid = threadIdx.x;
+  const size_t N = (size_t)nx * ny * nz;
+  double e = 0.0, w = 0.0;
+  for (size_t n = (size_t)blockIdx.x * blockDim.x + tid; n < N; n += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(n % nx), y = (int)((n / nx) % ny), z = (int)(n / ((size_t)nx * ny));
+    const size_t sy = nx, sz = (size_t)nx * ny;
+    const size_t xm = n - x + (x == 0 ? nx - 1 : x - 1), xp = n - x + (x + 1 == nx ? 0 : x + 1);
+    const size_t ym = n + ((y == 0 ? ny - 1 : y - 1) - y) * sy, yp = n + ((y + 1 == ny ? 0 : y + 1) - y) * sy;
+    const size_t zm = n + ((z == 0 ? nz - 1 : z - 1) - z) * sz, zp = n + ((z + 1 == nz ? 0 : z + 1) - z) * sz;
+    const double ux = u[3 * n], uy = u[3 * n + 1], uz = u[3 * n + 2];
+    e += 0.5 * (ux * ux + uy * uy + uz * uz);
+    // d(u_c)/d(axis) = (u_c(+1) - u_c(-1)) / 2
+    const double duz_dy = 0.5 * ((double)u[3 * yp + 2] - (double)u[3 * ym + 2]);
+    const double duy_dz = nz > 1 ? 0.5 * ((double)u[3 * zp + 1] - (double)u[3 * zm + 1]) : 0.0;
+    const double dux_dz = nz > 1 ? 0.5 * ((double)u[3 * zp] - (double)u[3 * zm]) : 0.0;
+    const double duz_dx = 0.5 * ((double)u[3 * xp + 2] - (double)u[3 * xm + 2]);
+    const double duy_dx = 0.5 * ((double)u[3 * xp + 1] - (double)u[3 * xm + 1]);
+    const double dux_dy = 0.5 * ((double)u[3 * yp] - (double)u[3 * ym]);
+    const double wx = duz_dy - duy_dz, wy = dux_dz - duz_dx, wz = duy_dx - dux_dy;
+    w += 0.5 * (wx * wx + wy * wy + wz * wz);
+  }
+  sh[0][tid] = e;
+  sh[1][tid] = w;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s) {
+      sh[0][tid] += sh[0][tid + s];
+      sh[1][tid] += sh[1][tid + s];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    atomicAdd(out, sh[0][0]);
+    atomicAdd(out + 1, sh[1][0]);
+  }
 }
 
 }  // namespace tclb

@@ -93,43 +93,39 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
 }
 
 // Issue the copies of tile t into one stage; called by the whole producer
-// warp after lane 0 has armed the stage's full barrier. A tile of R > 1 rows
-// (nx <= 256) takes one R-row box per population; a one-row tile (nx up to
-// 512) takes its row as nb boxes of nx/nb values. Copy c = (field, box) goes
-// to lane c mod 32; field Q is the node types.
+// warp after lane 0 has armed the stage's full barrier. Lane i < Q copies
+// population i (one R-row box, or R one-row boxes where the rows wrap at a
+// y face), lane Q the node types.
 template <class M>
 __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage, unsigned bar, int t, int nx,
-                                         int ny, int nz, int R, int nb, int lane) {
+                                         int ny, int nz, int R, int lane) {
   const int rows_per_plane = ny / R;
   const int z = t / rows_per_plane, y0 = (t % rows_per_plane) * R;
   const unsigned block = (unsigned)R * nx;  // values per population block
-  const int bw = nx / nb;                   // box width
-  for (int c = lane; c < (M::Q + 1) * nb; c += 32) {
-    const int i = c / nb, xb = (c % nb) * bw;
-    if (i == M::Q) {
-      tma_load_3d(smem_u32(stage + (size_t)M::Q * block + xb), &T.flags, xb, y0, z, bar);
-      continue;
-    }
+  if (lane < M::Q) {
+    const int i = lane;
     const int ey = M::ey(i), ez = M::DIM == 2 ? 0 : M::ez(i);
     int zs = z - ez;
     zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
-    const unsigned dst = smem_u32(stage + (size_t)i * block + xb);
+    const unsigned dst = smem_u32(stage + (size_t)i * block);
     const int ys = y0 - ey;
-    if (R > 1 && ys >= 0 && ys + R <= ny) {
-      tma_load_4d(dst, &T.rows, xb, ys, zs, i, bar);
-    } else {  // one row at a time (one-row tiles, and rows that wrap at a y face)
+    if (ys >= 0 && ys + R <= ny) {
+      tma_load_4d(dst, &T.rows, 0, ys, zs, i, bar);
+    } else {  // rows wrap at a y face: one row at a time
       for (int r = 0; r < R; r++) {
         int y = ys + r;
         y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-        tma_load_4d(dst + (unsigned)(r * nx * 2), &T.row1, xb, y, zs, i, bar);
+        tma_load_4d(dst + (unsigned)(r * nx * 2), &T.row1, 0, y, zs, i, bar);
       }
     }
+  } else if (lane == M::Q) {
+    tma_load_3d(smem_u32(stage + (size_t)M::Q * block), &T.flags, 0, y0, z, bar);
   }
 }
 
-// The kernel: ncons = R*nx/64 warps (at most TMA_CONSUMERS) update node
-// pairs, one more warp (the last) produces. Block = (ncons + 1) * 32 threads;
-// the consumer warps cover the tile's R*nx/2 pairs, one pair per thread. Grid = resident blocks
+// The kernel: ncons = R*nx/64 = TMA_CONSUMERS warps update node pairs, one
+// more warp (the last) produces. Block = (ncons + 1) * 32 threads; the
+// consumer warps cover the tile's R*nx/2 pairs, one pair per thread. Grid = resident blocks
 // (persistent), walking tiles t = blockIdx.x + k*gridDim.x.
 // Dynamic shared memory: 128 bytes of mbarriers (full[S], empty[S]), then
 // TMA_STAGES stages.
@@ -139,7 +135,7 @@ constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
 template <class M, class R, class St>
 __global__ void __launch_bounds__(TMA_THREADS, 2)
     k_iterate_tma(const Args<R, M::NSET> a, const __grid_constant__ TmaMaps T,
-                  const PlaneAddr<typename St::T, M::Q> P, int R_rows, int nb, int* err) {
+                  const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err) {
   static_assert(M::Q < 32, "one producer lane per population plus one for the node types");
   using P16 = Pack16<St>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -181,7 +177,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
         mbar_expect_tx(fb, (unsigned)(M::Q + 1) * block * 2u);
       }
       __syncwarp();
-      tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, nb, lane);
+      tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);
     }
     return;
   }

@@ -160,7 +160,7 @@ struct tclb_lattice {
   int use_pairs = 1;  // 16-bit storage: two nodes per thread when nx % 64 == 0
   // 16-bit storage: tile-staged TMA kernel (tma_rows rows per tile; tma[b]
   // describes snapshot b as the source), and its error word in the pool
-  int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_boxes = 1, tma_grid = 0;
+  int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_grid = 0;
   TmaMaps tma[2];
   int* err_dev = nullptr;
 };
@@ -221,8 +221,7 @@ struct Launch {
         const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
         const size_t smem = 128 + (size_t)TMA_STAGES * (M::Q + 1) * rows * L->nx * sizeof(T);
         if (L->tma_grid > 0) {
-          k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->tma_boxes,
-                                                                     L->err_dev);
+          k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev);
           return;
         }
       }
@@ -347,19 +346,18 @@ EncodeTiledFn encode_tiled() {
 
 void setup_tma(tclb_lattice* L) {
   L->tma_ok = 0;
-  if (L->elem != 2 || L->nx % 64 || L->nx > 512 || (L->nx > 256 && L->nx % 128)) return;
-  // tiles of 512 nodes (R rows) up to nx = 256; one-row tiles of two boxes above
-  const int R = L->nx <= 256 ? 512 / L->nx : 1;
-  const int nb = L->nx <= 256 ? 1 : 2;
+  // Tiles of 512 nodes (R whole rows). Longer rows take the register pair
+  // kernel: one-row tiles copied in two boxes measured slower than it.
+  if (L->elem != 2 || L->nx % 64 || L->nx > 256) return;
+  const int R = 512 / L->nx;
   if (L->ny % R) return;
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return;
   const cuuint64_t e = 2;
   const cuuint64_t dims[4] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz, (cuuint64_t)L->T->Q};
   const cuuint64_t strides[3] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e, L->stride * e};
-  const cuuint32_t bw = (cuuint32_t)(L->nx / nb);
-  const cuuint32_t box_rows[4] = {bw, (cuuint32_t)R, 1, 1};
-  const cuuint32_t box_row1[4] = {bw, 1, 1, 1};
+  const cuuint32_t box_rows[4] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1, 1};
+  const cuuint32_t box_row1[4] = {(cuuint32_t)L->nx, 1, 1, 1};
   const cuuint32_t ones[4] = {1, 1, 1, 1};
   for (int b = 0; b < 2; b++) {
     if (enc(&L->tma[b].rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, L->buf[b], dims, strides, box_rows, ones,
@@ -372,14 +370,13 @@ void setup_tma(tclb_lattice* L) {
       return;
     const cuuint64_t fdims[3] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz};
     const cuuint64_t fstrides[2] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e};
-    const cuuint32_t fbox[3] = {bw, (cuuint32_t)R, 1};
+    const cuuint32_t fbox[3] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1};
     if (enc(&L->tma[b].flags, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, L->flags, fdims, fstrides, fbox, ones,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return;
   }
   L->tma_rows = R;
-  L->tma_boxes = nb;
   L->tma_ok = 1;
 }
 
@@ -777,6 +774,38 @@ int tclb_get_quantity(tclb_h L, int q, const int region[6], void* out, double sc
   L->impl->quantity(L, q, vec, r, scale, L->qbuf, s);
   TCLB_CK(cudaGetLastError());
   TCLB_CK(cudaMemcpyAsync(out, L->qbuf, bytes, cudaMemcpyDeviceToHost, s));
+  TCLB_CK(cudaStreamSynchronize(s));
+  return TCLB_OK;
+}
+
+int tclb_energy_enstrophy(tclb_h L, double* out, void* stream) {
+  CHECK_H(L);
+  if (!out) return fail(TCLB_ERR_ARG, "null output");
+  int q = -1;
+  for (int i = 0; i < L->T->nquantities; i++)
+    if (std::strcmp(L->T->quantity_names[i], "U") == 0) q = i;
+  if (q < 0) return fail(TCLB_ERR_ARG, "model has no U quantity");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : L->stream;
+  const size_t ub = align_up(3 * L->N * L->impl->real_size, 256);
+  const size_t bytes = ub + 256;
+  if (bytes > L->qbuf_bytes) {
+    if (L->qbuf) TCLB_CK(cudaFree(L->qbuf));
+    L->qbuf = nullptr;
+    L->qbuf_bytes = 0;
+    TCLB_CK(cudaMalloc(&L->qbuf, bytes));
+    L->qbuf_bytes = bytes;
+  }
+  const int r[6] = {0, 0, 0, L->nx, L->ny, L->nz};
+  L->impl->quantity(L, q, 1, r, 1.0, L->qbuf, s);
+  double* acc = reinterpret_cast<double*>(static_cast<char*>(L->qbuf) + ub);
+  TCLB_CK(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+  const int blocks = (int)std::min<size_t>((L->N + 255) / 256, 148 * 8);
+  if (L->precision == TCLB_FP64)
+    k_energy_enstrophy<double><<<blocks, 256, 0, s>>>(static_cast<const double*>(L->qbuf), L->nx, L->ny, L->nz, acc);
+  else
+    k_energy_enstrophy<float><<<blocks, 256, 0, s>>>(static_cast<const float*>(L->qbuf), L->nx, L->ny, L->nz, acc);
+  TCLB_CK(cudaGetLastError());
+  TCLB_CK(cudaMemcpyAsync(out, acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   TCLB_CK(cudaStreamSynchronize(s));
   return TCLB_OK;
 }

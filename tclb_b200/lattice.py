@@ -78,6 +78,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_load_pri.argtypes = [h, vp, sz]
     L.tclb_color.argtypes = [h, vp, i, i, vp]
     L.tclb_get_launch.argtypes = [h, ip, ip, ip]
+    L.tclb_energy_enstrophy.argtypes = [h, dp, vp]
     _lib = L
     return L
 
@@ -271,6 +272,12 @@ class Lattice:
 
     def sync(self):
         _check(self.lib.tclb_sync(self._h))
+
+    def energy_enstrophy(self, stream: int = 0) -> tuple:
+        """(kinetic energy 1/2 sum |U|^2, enstrophy 1/2 sum |curl U|^2), FP64, lattice units."""
+        out = np.zeros(2)
+        _check(self.lib.tclb_energy_enstrophy(self._h, _dp(out), ctypes.c_void_p(stream or None)))
+        return float(out[0]), float(out[1])
 
     def launch_path(self) -> dict:
         """The paths plain iterations take: graphs, pairs, tma (enabled and applicable)."""
