@@ -116,7 +116,7 @@ struct D2Q9 {
   __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
   template <class R>
   __device__ __forceinline__ static void pre_collision(R (&)[Q], flag_t, const Args<R, NSET>&) {}
-  template <class R>
+  template <bool DEV, class R>
   __device__ __forceinline__ static void collide_pair(F2 (&)[Q], flag_t, flag_t, const Args<R, NSET>&) {}
   template <class R>
   __host__ __device__ static void derived(const R*, R* k) { k[0] = k[1] = k[2] = k[3] = R(0); }
@@ -409,8 +409,11 @@ struct D3Q19 {
   // with even/odd parts taken over each pair (i, opposite i). It is evaluated
   // that way here: pair sums and differences instead of two 19x19 transforms.
   // The two-rate update for value type V (R, or F2 for two nodes); leaves
-  // rho and the forced momentum J' for the Globals.
-  template <class V, class R>
+  // rho and the forced momentum J' for the Globals. With DEV the values are
+  // deviations g = f - w: the sum of g is rho - 1, which enters the
+  // equilibrium's terms linear in rho (giving feq - w), while the quadratic
+  // terms and the force use the true density.
+  template <bool DEV = false, class V, class R>
   __device__ __forceinline__ static void trt(V (&f)[Q], const Args<R, NSET>& a, V& rho, V& jx, V& jy, V& jz) {
     V s[9], d[9];
 #pragma unroll
@@ -423,12 +426,13 @@ struct D3Q19 {
     jy = d[1] + d[3] + d[4] + d[7] - d[8];
     jz = d[2] + d[5] + d[6] + d[7] + d[8];
     const V g1 = V(a.k[0]), g2 = V(a.k[1]);
-    const V irho = recip(rho);
+    const V rho_t = DEV ? rho + V(1) : rho;  // true density
+    const V irho = recip(rho_t);
     V e0, e[9], o[9];
     feq_parts(rho, irho, jx, jy, jz, e0, e, o);
-    jx += rho * V(a.s[d3q19::S_ForceX]);
-    jy += rho * V(a.s[d3q19::S_ForceY]);
-    jz += rho * V(a.s[d3q19::S_ForceZ]);
+    jx += rho_t * V(a.s[d3q19::S_ForceX]);
+    jy += rho_t * V(a.s[d3q19::S_ForceY]);
+    jz += rho_t * V(a.s[d3q19::S_ForceZ]);
     V e0n, en[9], on[9];
     feq_parts(rho, irho, jx, jy, jz, e0n, en, on);
     f[0] = e0n + g1 * (f[0] - e0);
@@ -535,10 +539,10 @@ struct D3Q19 {
   __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
     boundaries(f, fl, a);
   }
-  template <class R>
+  template <bool DEV, class R>
   __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const Args<R, NSET>& a) {
     F2 rho, jx, jy, jz;
-    trt(f, a, rho, jx, jy, jz);
+    trt<DEV>(f, a, rho, jx, jy, jz);
   }
 
   // SetEquilibrum (:212-217): f = Req(rho, J) . MRTMAT.inv
@@ -766,12 +770,30 @@ struct D3Q27C {
       boundaries<R, false>(f, fl, g, a.zone + (fl >> ZONE_SHIFT) * NZS);
     }
   }
-  template <class R>
+  // With DEV the values are deviations g = f - w. The raw-moment transform is
+  // linear, so the weights' raw moments (per axis (1, 0, 1/3): m000 = 1,
+  // m200 = m020 = m002 = 1/3, m220 = m202 = m022 = 1/9, m222 = 1/27) are added
+  // after the forward transform and taken off before the backward one,
+  // instead of adding and removing w on all 27 populations.
+  template <class V>
+  __device__ __forceinline__ static void weight_moments(V (&m)[Q], float sign) {
+    m[0] += V(sign);
+    m[2] += V(sign * (1.0f / 3.0f));
+    m[6] += V(sign * (1.0f / 3.0f));
+    m[18] += V(sign * (1.0f / 3.0f));
+    m[8] += V(sign * (1.0f / 9.0f));
+    m[20] += V(sign * (1.0f / 9.0f));
+    m[24] += V(sign * (1.0f / 9.0f));
+    m[26] += V(sign * (1.0f / 27.0f));
+  }
+  template <bool DEV, class R>
   __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t fla, flag_t flb, const Args<R, NSET>& a) {
     const F2 w0((float)((fla & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]), (float)((flb & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]));
     to_raw(f);
+    if (DEV) weight_moments(f, 1.0f);
     if (a.s[d3q27c::S_Omega] == R(1)) relax<F2, R, false>(f, a, w0);
     else relax<F2, R, true>(f, a, w0);
+    if (DEV) weight_moments(f, -1.0f);
     from_raw(f);
   }
 
@@ -1017,24 +1039,27 @@ __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla,
     // its lane taken out, updated by the scalar boundary code and put back;
     // then one packed FP32x2 collision serves both nodes, so bulk and
     // boundary pairs do not diverge in the collision.
+    // With shifted storage the packed values stay deviations g = f - w
+    // (the collision works on them directly); the scalar boundary code sees f.
+    constexpr float SH = St::shifted ? 1.0f : 0.0f;
     F2 f2[M::Q];
 #pragma unroll
-    for (int i = 0; i < M::Q; i++) f2[i] = St::shifted ? F2(v[i]) + F2(M::w(i)) : F2(v[i]);
+    for (int i = 0; i < M::Q; i++) f2[i] = F2(v[i]);
     if (M::has_boundary(fla)) {
       float t[M::Q];
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.x;
+      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.x + SH * (float)M::w(i);
       M::pre_collision(t, fla, a);
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) f2[i].v.x = t[i];
+      for (int i = 0; i < M::Q; i++) f2[i].v.x = t[i] - SH * (float)M::w(i);
     }
     if (M::has_boundary(flb)) {
       float t[M::Q];
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.y;
+      for (int i = 0; i < M::Q; i++) t[i] = f2[i].v.y + SH * (float)M::w(i);
       M::pre_collision(t, flb, a);
 #pragma unroll
-      for (int i = 0; i < M::Q; i++) f2[i].v.y = t[i];
+      for (int i = 0; i < M::Q; i++) f2[i].v.y = t[i] - SH * (float)M::w(i);
     }
     const bool ca = M::collides(fla), cb = M::collides(flb);
     if (ca || cb) {
@@ -1048,7 +1073,7 @@ __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla,
 #pragma unroll
         for (int i = 0; i < M::Q; i++) keep[i] = ca ? f2[i].v.y : f2[i].v.x;
       }
-      M::collide_pair(f2, fla, flb, a);
+      M::template collide_pair<St::shifted>(f2, fla, flb, a);
       if (mixed) {
 #pragma unroll
         for (int i = 0; i < M::Q; i++) {
@@ -1058,7 +1083,7 @@ __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla,
       }
     }
 #pragma unroll
-    for (int i = 0; i < M::Q; i++) v[i] = St::shifted ? (f2[i] - F2(M::w(i))).v : f2[i].v;
+    for (int i = 0; i < M::Q; i++) v[i] = f2[i].v;
   } else {
     R fa[M::Q], fb[M::Q];
 #pragma unroll
