@@ -42,6 +42,7 @@ struct BatchImpl {
   void (*clear)(BatchCase*, int, cudaStream_t);
   void (*init)(const BatchCase&, const void* dst, cudaStream_t, int bx, int by);
   void (*quantity)(const BatchCase&, int parity, int q, int vec, double scale, void* out, cudaStream_t);
+  int (*blocks_per_sm)(int threads);
   size_t real_size;
   int Q, NG, NSET, NZS, zone_shift;
 };
@@ -65,9 +66,21 @@ Args<R, M::NSET> args_of(const BatchCase& C, const void* src, void* dst) {
 
 template <class M, class R, class St>
 struct BL {
+  // launch K-1 of a replay is every case's last iteration: the Globals variant
   static void iterate(const BatchCase* c, const BatchTile* t, const int* n, int k, int K, dim3 g, dim3 b,
                       cudaStream_t s) {
-    k_iterate_batch<M, R, St><<<g, b, 0, s>>>(c, t, n, k, K);
+    if (k == K - 1) k_iterate_batch<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
+    else k_iterate_batch<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
+  }
+  // resident blocks per SM of the plain kernel at this block size
+  static int blocks_per_sm(int threads) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_iterate_batch<M, R, St, false>, threads, 0) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return n;
   }
   static void clear(BatchCase* c, int n, cudaStream_t s) {
     if (n > 0) k_batch_clear_globals<M::NG><<<n, 32, 0, s>>>(c, n);
@@ -84,8 +97,8 @@ struct BL {
                                                       static_cast<R*>(out));
   }
   static const BatchImpl* get() {
-    static const BatchImpl impl = {iterate, clear, init, quantity, sizeof(R), M::Q, M::NG, M::NSET, M::NZS,
-                                   M::ZONE_SHIFT};
+    static const BatchImpl impl = {iterate, clear, init, quantity, blocks_per_sm, sizeof(R), M::Q, M::NG, M::NSET,
+                                   M::NZS, M::ZONE_SHIFT};
     return &impl;
   }
 };
@@ -202,7 +215,8 @@ int ensure_graph(tclb_batch* B) {
   }
   int dev = B->device, sms = 148, per_sm = 4;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  per_sm = std::max(1, 2048 / (B->bx * B->by));
+  per_sm = B->I->blocks_per_sm(B->bx * B->by);
+  if (per_sm < 1) per_sm = std::max(1, 2048 / (B->bx * B->by));
   B->grid_blocks = B->user_grid > 0 ? B->user_grid : sms * per_sm;
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));

@@ -11,10 +11,15 @@
 // multiple of 32 (TCLB's padding) a tile width of 32 leaves no thread idle on
 // any case; wider tiles trade that for fewer tiles. The autotuner chooses.
 //
-// A launch is iteration k (0-based) of a replay of K iterations. Case c runs
-// it when k < remaining[c]; its A/B parity is (counter[c] + k) & 1. The
-// counters advance only in k_batch_advance at the end of a replay, so a CUDA
-// graph of K launches + advance can be replayed while cases come and go.
+// A launch is iteration k (0-based) of a replay of K iterations. A case with
+// d = min(remaining, K) iterations to do in this replay runs the last d
+// launches, k = K-d .. K-1, so every case's last iteration of a replay is
+// launch K-1: that launch alone is the Globals variant, and the plain
+// launches carry no Globals code (the register count of the one-lattice
+// kernel, not of both paths). Its A/B parity at launch k is
+// (counter + k - (K - d)) & 1. The counters advance only in k_batch_advance
+// at the end of a replay, so a CUDA graph of K launches + advance can be
+// replayed while cases come and go.
 #pragma once
 #include "lbm_kernels.cuh"
 
@@ -39,7 +44,7 @@ struct BatchTile {
   int slot, x0, y0, z;
 };
 
-template <class M, class R, class St>
+template <class M, class R, class St, bool G>
 __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restrict__ cases,
                                                        const BatchTile* __restrict__ tiles,
                                                        const int* __restrict__ ntiles_p, int k, int K) {
@@ -50,7 +55,6 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
   const int nchunks = (ntiles + TILE_CHUNK - 1) / TILE_CHUNK;
   int slot = -1;
   bool skip = true;
-  int last = 0;
   Args<R, M::NSET> a;
   for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const int t_end = min(ntiles, (ch + 1) * TILE_CHUNK);
@@ -60,9 +64,10 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
         slot = tile.slot;
         const BatchCase& C = cases[slot];
         const int remaining = C.remaining;
-        skip = !C.active || k >= remaining;
-        last = (remaining < K ? remaining : K) - 1;
-        const int parity = (C.counter + k) & 1;
+        const int d = remaining < K ? remaining : K;  // this case's iterations in the replay
+        const int first = K - d;                      // it runs launches first .. K-1
+        skip = !C.active || d <= 0 || k < first;
+        const int parity = (C.counter + (k - first)) & 1;
         a.src = C.buf[parity];
         a.dst = C.buf[1 - parity];
         a.stride = C.stride;
@@ -81,16 +86,18 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
       const bool act = x < a.nx && y < a.ny;
       using T = typename St::T;
       const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
-      if (k == last) {
+      if constexpr (G) {
         R g[M::NG];
 #pragma unroll
         for (int i = 0; i < M::NG; i++) g[i] = 0;
         if (act) node_update<M, R, St, true>(a, P, x, y, z, g);
         reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
         __syncthreads();  // shared scratch of reduce_globals reused by the next tile
-      } else if (act) {
-        R g[1];
-        node_update<M, R, St, false>(a, P, x, y, z, g);
+      } else {
+        if (act) {
+          R g[1];
+          node_update<M, R, St, false>(a, P, x, y, z, g);
+        }
       }
     }
   }

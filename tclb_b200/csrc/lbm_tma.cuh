@@ -37,7 +37,13 @@ struct TmaMaps {
   CUtensorMap flags;  // node types: dims (nx, ny, nz), box (nx, R, 1)
 };
 
-constexpr int TMA_STAGES = 3;
+// Stages (shared memory per block: 128 + 3 * (Q+1) * 1 KB), two blocks per
+// SM. Three suffice: for d3q19, whose tiles compute fastest, 4 and 5 stages
+// measured the same.
+template <class M>
+constexpr int tma_stages() {
+  return 3;
+}
 constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
 constexpr int TMA_ERR_TIMEOUT = 1;
 
@@ -140,7 +146,9 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   using P16 = Pack16<St>;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);
-  unsigned long long* empty = full + TMA_STAGES;
+  constexpr int TMA_STAGES = tma_stages<M>();
+  static_assert(TMA_STAGES <= 8, "128 bytes hold 8 full and 8 empty barriers");
+  unsigned long long* empty = full + 8;
   unsigned short* stages = reinterpret_cast<unsigned short*>(smem + 128);
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const unsigned block = (unsigned)R_rows * nx;
