@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--rate", type=float, default=6.0, help="config 5: Poisson arrival rate (requests/s)")
     p.add_argument("--path", default="auto", choices=["auto", "tma", "pairs", "one"],
                    help="16-bit storage kernel for plain iterations: auto (tile-staged TMA where it "
                         "applies, else two nodes per thread), tma, pairs, one (one node per thread)")
@@ -366,7 +367,7 @@ def run_config(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     fn = {1: BM.config1, 3: BM.config3, 4: BM.config4, 5: BM.config5}[args.config]
-    res = fn()
+    res = fn(rate=args.rate) if args.config == 5 else fn()
     print(json.dumps({"metric": METRIC, "unit": UNIT, "config_id": args.config, "data": "synthetic", **res}),
           flush=True)
     return 0

@@ -239,8 +239,15 @@ int tclb_batch_add_case(tclb_batch_h b, int nx, int ny, int nz, const uint16_t* 
 int tclb_batch_remove_case(tclb_batch_h b, int case_id);
 
 /* Launch shape: tile bx x by nodes per block (bx multiple of 32, bx*by <= 256),
-   iterations per replay, persistent grid size (0 = SMs x resident blocks). */
+   iterations per replay, and grid: 0 (default) = one block per tile, > 0 = a
+   persistent grid of that many blocks walking the tiles, < 0 = persistent with
+   SMs x resident blocks. One block per tile measured fastest on mixed sizes. */
 int tclb_batch_set_launch(tclb_batch_h b, int bx, int by, int iters_per_launch, int grid_blocks);
+/* Run the batch's work on a high-priority stream (high != 0) or a normal one:
+   with batches of different models running at once, the blocks of the
+   high-priority batch are scheduled first (e.g. small cases that should not
+   wait behind large ones). Waits for the batch's work in flight. */
+int tclb_batch_set_priority(tclb_batch_h b, int high);
 int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launch);
 
 /* Enqueue one replay (asynchronous); every active case advances by
@@ -248,6 +255,9 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    last iteration in the replay. */
 int tclb_batch_step(tclb_batch_h b);
 int tclb_batch_sync(tclb_batch_h b);
+/* 1 when the batch's enqueued work has finished (tclb_batch_sync then returns
+   at once), 0 while it runs, negative on error; never blocks. */
+int tclb_batch_done(tclb_batch_h b);
 /* After tclb_batch_sync: iterations done / left for a case. */
 int tclb_batch_poll(tclb_batch_h b, int case_id, long long* iterations_done, int* remaining);
 int tclb_batch_get_globals(tclb_batch_h b, int case_id, double* out);

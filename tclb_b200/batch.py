@@ -39,6 +39,8 @@ def _lib():
         L.tclb_batch_get_launch.argtypes = [h, ip, ip, ip]
         L.tclb_batch_step.argtypes = [h]
         L.tclb_batch_sync.argtypes = [h]
+        L.tclb_batch_done.argtypes = [h]
+        L.tclb_batch_set_priority.argtypes = [h, i]
         L.tclb_batch_poll.argtypes = [h, i, ctypes.POINTER(ctypes.c_longlong), ip]
         L.tclb_batch_get_globals.argtypes = [h, i, dp]
         L.tclb_batch_get_quantity.argtypes = [h, i, i, vp, d]
@@ -157,6 +159,17 @@ class Batch:
 
     def sync(self):
         _check(self.lib.tclb_batch_sync(self._h))
+
+    def set_priority(self, high: bool):
+        """Schedule this batch's blocks ahead of normal-priority batches."""
+        _check(self.lib.tclb_batch_set_priority(self._h, 1 if high else 0))
+
+    def done(self) -> bool:
+        """True when the enqueued replays have finished (never blocks)."""
+        rc = self.lib.tclb_batch_done(self._h)
+        if rc < 0:
+            _check(rc)
+        return rc == 1
 
     def poll(self, cid: int) -> Tuple[int, int]:
         done, rem = ctypes.c_longlong(), ctypes.c_int()

@@ -38,11 +38,12 @@ int bfail(int code, const std::string& msg) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct BatchImpl {
-  void (*iterate)(const BatchCase*, const BatchTile*, const int*, int, int, dim3, dim3, cudaStream_t);
+  void (*iterate)(const BatchCase*, const BatchTile*, const int*, int, int, dim3, dim3, bool, cudaStream_t);
   void (*clear)(BatchCase*, int, cudaStream_t);
   void (*init)(const BatchCase&, const void* dst, cudaStream_t, int bx, int by);
   void (*quantity)(const BatchCase&, int parity, int q, int vec, double scale, void* out, cudaStream_t);
   int (*blocks_per_sm)(int threads);
+  const void* (*tile_kernel)(bool globals);
   size_t real_size;
   int Q, NG, NSET, NZS, zone_shift;
 };
@@ -68,9 +69,18 @@ template <class M, class R, class St>
 struct BL {
   // launch K-1 of a replay is every case's last iteration: the Globals variant
   static void iterate(const BatchCase* c, const BatchTile* t, const int* n, int k, int K, dim3 g, dim3 b,
-                      cudaStream_t s) {
-    if (k == K - 1) k_iterate_batch<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
-    else k_iterate_batch<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
+                      bool per_tile, cudaStream_t s) {
+    if (per_tile) {
+      if (k == K - 1) k_iterate_batch_tile<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
+      else k_iterate_batch_tile<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
+    } else {
+      if (k == K - 1) k_iterate_batch<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
+      else k_iterate_batch<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
+    }
+  }
+  static const void* tile_kernel(bool globals) {
+    return globals ? reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, true>)
+                   : reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, false>);
   }
   // resident blocks per SM of the plain kernel at this block size
   static int blocks_per_sm(int threads) {
@@ -97,8 +107,8 @@ struct BL {
                                                       static_cast<R*>(out));
   }
   static const BatchImpl* get() {
-    static const BatchImpl impl = {iterate, clear, init, quantity, blocks_per_sm, sizeof(R), M::Q, M::NG, M::NSET,
-                                   M::NZS, M::ZONE_SHIFT};
+    static const BatchImpl impl = {iterate, clear, init, quantity, blocks_per_sm, tile_kernel, sizeof(R), M::Q,
+                                   M::NG, M::NSET, M::NZS, M::ZONE_SHIFT};
     return &impl;
   }
 };
@@ -172,7 +182,10 @@ struct tclb_batch {
   int ntiles = 0;
   int bx = 128, by = 2, K = 16, grid_blocks = 0, user_grid = 0;
   cudaGraphExec_t graph = nullptr;
-  int graph_key[4] = {-1, -1, -1, -1};
+  cudaGraph_t graph_src = nullptr;            // kept: its nodes address the instantiated graph
+  std::vector<cudaGraphNode_t> iter_nodes;    // the K iteration launches (one block per tile)
+  int graph_grid = 0;                         // their grid size in the instantiated graph
+  int graph_key[5] = {-1, -1, -1, -1, -1};
 };
 
 namespace {
@@ -206,25 +219,49 @@ int rebuild_tiles(tclb_batch* B) {
   return TCLB_OK;
 }
 
+// One block per tile: the iteration launches' grid is the live tile count.
+// When only that changes, the K kernel nodes of the instantiated graph get
+// the new grid in place (no recapture).
+int update_graph_grid(tclb_batch* B) {
+  const int grid = std::max(1, B->ntiles);
+  if (B->user_grid != 0 || grid == B->graph_grid) return TCLB_OK;
+  for (cudaGraphNode_t node : B->iter_nodes) {
+    cudaKernelNodeParams p;
+    BCK(cudaGraphKernelNodeGetParams(node, &p));
+    p.gridDim = dim3(grid);
+    BCK(cudaGraphExecKernelNodeSetParams(B->graph, node, &p));
+  }
+  B->graph_grid = grid;
+  return TCLB_OK;
+}
+
 int ensure_graph(tclb_batch* B) {
-  const int key[4] = {B->bx, B->by, B->K, (int)B->cases.size()};
-  if (B->graph && std::equal(key, key + 4, B->graph_key)) return TCLB_OK;
+  const int key[5] = {B->bx, B->by, B->K, (int)B->cases.size(), B->user_grid};
+  if (B->graph && std::equal(key, key + 5, B->graph_key)) return update_graph_grid(B);
   if (B->graph) {
     cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
   }
+  if (B->graph_src) {
+    cudaGraphDestroy(B->graph_src);
+    B->graph_src = nullptr;
+  }
+  B->iter_nodes.clear();
   int dev = B->device, sms = 148, per_sm = 4;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   per_sm = B->I->blocks_per_sm(B->bx * B->by);
   if (per_sm < 1) per_sm = std::max(1, 2048 / (B->bx * B->by));
-  B->grid_blocks = B->user_grid > 0 ? B->user_grid : sms * per_sm;
+  // grid_blocks 0 (default): one block per live tile; > 0: a persistent grid
+  // of that size walking the tiles; < 0: persistent, SMs x resident blocks.
+  const bool per_tile = B->user_grid == 0;
+  B->grid_blocks = per_tile ? std::max(1, B->ntiles) : (B->user_grid > 0 ? B->user_grid : sms * per_sm);
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   const int n = (int)B->cases.size();
   B->I->clear(B->d_cases, n, B->stream);
   for (int k = 0; k < B->K; k++)
     B->I->iterate(B->d_cases, B->d_tiles, B->d_ntiles, k, B->K, dim3(B->grid_blocks), dim3(B->bx, B->by),
-                  B->stream);
+                  per_tile, B->stream);
   if (n > 0) {
     k_batch_advance<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->K);
     k_batch_status<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->d_status);
@@ -232,9 +269,29 @@ int ensure_graph(tclb_batch* B) {
   cudaError_t e = cudaStreamEndCapture(B->stream, &g);
   if (e != cudaSuccess) return bfail(TCLB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   e = cudaGraphInstantiate(&B->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return bfail(TCLB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-  std::copy(key, key + 4, B->graph_key);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return bfail(TCLB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  B->graph_src = g;
+  if (per_tile) {  // remember the iteration launches, to resize their grid later
+    size_t count = 0;
+    BCK(cudaGraphGetNodes(g, nullptr, &count));
+    std::vector<cudaGraphNode_t> nodes(count);
+    BCK(cudaGraphGetNodes(g, nodes.data(), &count));
+    const void* f0 = B->I->tile_kernel(false);
+    const void* f1 = B->I->tile_kernel(true);
+    for (cudaGraphNode_t node : nodes) {
+      cudaGraphNodeType type;
+      BCK(cudaGraphNodeGetType(node, &type));
+      if (type != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams p;
+      BCK(cudaGraphKernelNodeGetParams(node, &p));
+      if (p.func == f0 || p.func == f1) B->iter_nodes.push_back(node);
+    }
+  }
+  B->graph_grid = B->grid_blocks;
+  std::copy(key, key + 5, B->graph_key);
   return TCLB_OK;
 }
 
@@ -296,6 +353,7 @@ int tclb_batch_destroy(tclb_batch_h B) {
   CHECK_B(B);
   if (B->stream) cudaStreamSynchronize(B->stream);
   if (B->graph) cudaGraphExecDestroy(B->graph);
+  if (B->graph_src) cudaGraphDestroy(B->graph_src);
   for (size_t s = 0; s < B->cases.size(); s++)
     if (B->used_slot[s]) cudaFreeAsync(B->cases[s].buf[0], B->stream);
   if (B->d_tiles) cudaFreeAsync(B->d_tiles, B->stream);
@@ -396,6 +454,18 @@ int tclb_batch_remove_case(tclb_batch_h B, int id) {
   return TCLB_OK;
 }
 
+int tclb_batch_set_priority(tclb_batch_h B, int high) {
+  CHECK_B(B);
+  int least = 0, greatest = 0;
+  BCK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  BCK(cudaStreamSynchronize(B->stream));  // pool allocations made on the old stream are complete
+  cudaStream_t s = nullptr;
+  BCK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high ? greatest : least));
+  cudaStreamDestroy(B->stream);
+  B->stream = s;
+  return TCLB_OK;
+}
+
 int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, int grid_blocks) {
   CHECK_B(B);
   if (bx < 32 || bx % 32 || by < 1 || bx * by > 256 || iters_per_launch < 1 || iters_per_launch > 4096)
@@ -404,7 +474,7 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
   B->bx = bx;
   B->by = by;
   B->K = iters_per_launch;
-  B->user_grid = grid_blocks > 0 ? grid_blocks : 0;
+  B->user_grid = grid_blocks;
   B->graph_key[0] = -1;
   return TCLB_OK;
 }
@@ -429,6 +499,14 @@ int tclb_batch_step(tclb_batch_h B) {
   BCK(cudaMemcpyAsync(B->h_status, B->d_status, sizeof(int2) * B->cases.size(), cudaMemcpyDeviceToHost,
                       B->stream));
   return TCLB_OK;
+}
+
+int tclb_batch_done(tclb_batch_h B) {
+  if (!B) return bfail(TCLB_ERR_ARG, "null batch handle");
+  const cudaError_t e = cudaStreamQuery(B->stream);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  return bfail(TCLB_ERR_CUDA, std::string("stream query: ") + cudaGetErrorString(e));
 }
 
 int tclb_batch_sync(tclb_batch_h B) {

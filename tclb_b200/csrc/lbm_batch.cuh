@@ -1,10 +1,13 @@
-// Batched iteration of many independent lattices in one persistent launch.
+// Batched iteration of many independent lattices, one launch per iteration
+// for all of them.
 //
 // No counterpart in the reference: TCLB runs one lattice per process. Here
 // each case (lattice) has a device descriptor; the cases' nodes are cut into
-// uniform tiles (one thread block each) listed in a device tile table, and a
-// persistent grid walks the table with a grid stride, so uneven case sizes
-// balance across the SMs. The physics is the per-model node update of
+// uniform tiles listed in a device tile table. By default every tile is one
+// thread block (k_iterate_batch_tile), so uneven case sizes balance across
+// the SMs through the hardware block scheduler; a persistent grid walking
+// the table with a grid stride (k_iterate_batch) is the alternative, slower
+// on mixed sizes. The physics is the per-model node update of
 // lbm_kernels.cuh, unchanged.
 //
 // A tile is a bx x by block of nodes of one z plane of one case. With nx a
@@ -100,6 +103,50 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
         }
       }
     }
+  }
+}
+
+// One block per tile (grid = tile-table capacity; blocks past the live tiles
+// return at once): blocks are independent, as in the one-lattice kernel.
+template <class M, class R, class St, bool G>
+__global__ void __launch_bounds__(256) k_iterate_batch_tile(const BatchCase* __restrict__ cases,
+                                                            const BatchTile* __restrict__ tiles,
+                                                            const int* __restrict__ ntiles_p, int k, int K) {
+  const int t = blockIdx.x;
+  if (t >= *ntiles_p) return;
+  const BatchTile tile = tiles[t];
+  const BatchCase& C = cases[tile.slot];
+  const int remaining = C.remaining;
+  const int d = remaining < K ? remaining : K;
+  const int first = K - d;
+  if (!C.active || d <= 0 || k < first) return;
+  const int parity = (C.counter + (k - first)) & 1;
+  Args<R, M::NSET> a;
+  a.src = C.buf[parity];
+  a.dst = C.buf[1 - parity];
+  a.stride = C.stride;
+  a.flags = C.flags;
+  a.nx = C.nx;
+  a.ny = C.ny;
+  a.nz = C.nz;
+  a.zone = static_cast<const R*>(C.zone);
+  a.glob = C.glob;
+#pragma unroll
+  for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
+  M::template derived<R>(a.s, a.k);
+  const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
+  const bool act = x < a.nx && y < a.ny;
+  using T = typename St::T;
+  const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
+  if constexpr (G) {
+    R g[M::NG];
+#pragma unroll
+    for (int i = 0; i < M::NG; i++) g[i] = 0;
+    if (act) node_update<M, R, St, true>(a, P, x, y, z, g);
+    reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
+  } else if (act) {
+    R g[1];
+    node_update<M, R, St, false>(a, P, x, y, z, g);
   }
 }
 

@@ -2,11 +2,13 @@
 
 Requests (a case of some model: node types, settings, iterations) arrive over
 time. The loop admits queued requests in arrival order while their device
-footprint fits the memory budget, keeps admitted lattices resident, advances
-every resident case by one graph replay per round -- one batch per model, each
-on its own stream, so the models' work overlaps on the GPU -- retires finished
-cases (Globals and, on request, a quantity are read back) and immediately
-admits more. Time to solution = completion time - arrival time.
+footprint fits the memory budget and keeps admitted lattices resident. Each
+model has one batch on its own stream; the batches run independently: as soon
+as a batch's graph replay has finished (a non-blocking query), its finished
+cases are retired (Globals and, on request, a quantity are read back), waiting
+requests are admitted into it, and its next replay is enqueued -- so the
+models' work overlaps on the GPU and no batch waits for another. Time to
+solution = completion time - arrival time.
 
 No counterpart in the reference (TCLB runs one case per process).
 """
@@ -47,7 +49,8 @@ class Request:
 
 class Server:
     def __init__(self, models=("d2q9", "d3q19"), precision="fp32", storage="same", budget_bytes: int = 150 << 30,
-                 launch: Optional[Dict[str, Tuple[int, int, int]]] = None, max_cases: int = 4096):
+                 launch: Optional[Dict[str, Tuple[int, int, int]]] = None, max_cases: int = 4096,
+                 high_priority: Tuple[str, ...] = ("d2q9",)):
         self.precision, self.storage = precision, storage
         self.budget = int(budget_bytes)
         self.batches: Dict[str, Batch] = {}
@@ -56,6 +59,8 @@ class Server:
             b = Batch(m, precision, storage, budget_bytes=self.budget, max_cases=max_cases)
             if launch and m in launch:
                 b.set_launch(*launch[m])
+            if m in high_priority:  # small cases: their blocks go first
+                b.set_priority(True)
             self.batches[m] = b
         self.queue: Deque[Request] = deque()
         self.resident: Dict[Tuple[str, int], Request] = {}
@@ -77,22 +82,27 @@ class Server:
             raise AdmissionRefused(f"request {r.rid} needs more than the whole budget")
         self.queue.append(r)
 
-    def _admit(self):
+    def _admit(self, idle):
+        """Admit waiting requests in arrival order into idle batches while the
+        budget allows (first come, first served: the head of the queue waits
+        for memory, or for its batch's replay in flight)."""
         now = self.now()
         while self.queue and self.queue[0].arrival <= now:
             r = self.queue[0]
             fp = self.footprint(r)
-            if self.used + fp > self.budget:
-                break  # first-come first-served: wait until memory frees up
+            if self.used + fp > self.budget or not idle[r.model]:
+                break
             cid = self.batches[r.model].add_case(r.spec)
             self.queue.popleft()
             self.used += fp
             r.admitted = self.now()
             self.resident[(r.model, cid)] = r
 
-    def _retire(self):
+    def _retire(self, model):
+        b = self.batches[model]
         for (m, cid), r in list(self.resident.items()):
-            b = self.batches[m]
+            if m != model:
+                continue
             _done, rem = b.poll(cid)
             if rem > 0:
                 continue
@@ -105,33 +115,42 @@ class Server:
             del self.resident[(m, cid)]
             self.done.append(r)
 
-    def round(self) -> bool:
-        """Admit, advance every resident case by one replay, retire. Returns
-        False when there was nothing to run."""
-        self._admit()
-        active = [b for b in self.batches.values() if b.pending_updates() > 0]
-        t = time.perf_counter()
-        for b in active:
-            b.step()  # asynchronous, one stream per model
-        for b in active:
-            b.sync()
-        if active:
-            self.busy += time.perf_counter() - t
-        self._retire()
-        self.rounds += 1
-        return bool(active)
-
     def run(self, requests: List[Request], timeout_s: float = 600.0) -> dict:
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
         self.t0 = time.perf_counter()
+        inflight = {m: False for m in self.batches}
+        t_prev = time.perf_counter()
         while (self.queue or self.resident) and self.now() < timeout_s:
-            if not self.round():
-                # idle: wait for the next arrival
-                if self.queue:
+            progressed = False
+            for m, b in self.batches.items():
+                if inflight[m]:
+                    if not b.done():
+                        continue
+                    b.sync()  # returns at once: updates the case status
+                    inflight[m] = False
+                    self._retire(m)
+                    progressed = True
+            idle = {m: not f for m, f in inflight.items()}
+            self._admit(idle)
+            for m, b in self.batches.items():
+                if not inflight[m] and b.pending_updates() > 0:
+                    b.step()
+                    inflight[m] = True
+                    self.rounds += 1
+                    progressed = True
+            t = time.perf_counter()
+            if any(inflight.values()):
+                self.busy += t - t_prev  # GPU work was in flight during this interval
+            t_prev = t
+            if not progressed:
+                if not any(inflight.values()) and self.queue:
                     dt = self.queue[0].arrival - self.now()
                     if dt > 0:
                         time.sleep(min(dt, 0.005))
+                        t_prev = time.perf_counter()
+                else:
+                    time.sleep(20e-6)
         wall = self.now()
         return self.report(wall)
 
