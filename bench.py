@@ -200,6 +200,21 @@ def cpu_baseline(args, model_name, seconds, threads=None):
 
 
 # ---------------------------------------------------------------------------
+def workload_config(args, world: int) -> dict:
+    """The workload both arms report (the reference arm times bounded samples of it)."""
+    from tclb_b200 import models as M
+
+    m = M.get(args.model)
+    n = args.n
+    elem = 8 if args.precision == "fp64" else (4 if args.storage == "same" else 2)
+    snap_gb = m.Q * elem * n ** 3 / 1e9
+    return {"workload": f"{args.model} Taylor-Green vortex {n}^3 periodic, u0=0.05, nu={TGV_NU[args.model]:g}",
+            "model": args.model, "lattice": [n, n, n], "precision": args.precision, "storage": args.storage,
+            "iterations_per_step": args.log_every, "globals_every": args.log_every,
+            "energy_enstrophy_every": args.log_every,
+            "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % snap_gb, "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -222,8 +237,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": el / len(vals) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"{args.model} Taylor-Green {args.n}^3 sampled as {args.n}x{args.n}x{args.cpu_slab} "
-                                   f"slabs", "precision": args.precision, "l2": "n/a (CPU)"},
+            "config": workload_config(args, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -343,13 +357,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-                "config": {"workload": f"{args.model} Taylor-Green vortex {n}^3 periodic, u0=0.05, "
-                                       f"nu={TGV_NU[args.model]:g}",
-                           "model": args.model, "lattice": [n, n, n], "precision": args.precision,
-                           "storage": args.storage, "iterations_per_step": I, "globals_every": I,
-                           "energy_enstrophy_every": I,
-                           "l2": "inputs larger than L2 (2 x %.2f GB snapshots)" % (bpu / 2 * N / 1e9),
-                           "parallelism": f"replicas x{world}", "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")},
+                "config": workload_config(args, world),
+                "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one"),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": args.steps * (I + 2), "wall_s": wall,
                 "globals_last": dict({k: float(v) for k, v in glob.items()}, KineticEnergy=energy[0],
