@@ -44,6 +44,8 @@ template <class M>
 constexpr int tma_stages() {
   return 3;
 }
+constexpr int TMA_CONSUMERS = 8;                   // consumer warps per block
+constexpr unsigned TMA_TILE = TMA_CONSUMERS * 64;  // nodes per tile (two per consumer thread)
 constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
 constexpr int TMA_ERR_TIMEOUT = 1;
 
@@ -107,7 +109,7 @@ __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage
                                          int ny, int nz, int R, int lane) {
   const int rows_per_plane = ny / R;
   const int z = t / rows_per_plane, y0 = (t % rows_per_plane) * R;
-  const unsigned block = (unsigned)R * nx;  // values per population block
+  constexpr unsigned block = TMA_TILE;  // values per population block (R * nx)
   if (lane < M::Q) {
     const int i = lane;
     const int ey = M::ey(i), ez = M::DIM == 2 ? 0 : M::ez(i);
@@ -135,7 +137,6 @@ __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage
 // (persistent), walking tiles t = blockIdx.x + k*gridDim.x.
 // Dynamic shared memory: 128 bytes of mbarriers (full[S], empty[S]), then
 // TMA_STAGES stages.
-constexpr int TMA_CONSUMERS = 8;
 constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
 
 template <class M, class R, class St>
@@ -151,8 +152,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   unsigned long long* empty = full + 8;
   unsigned short* stages = reinterpret_cast<unsigned short*>(smem + 128);
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const unsigned block = (unsigned)R_rows * nx;
-  const size_t stage_elems = (size_t)(M::Q + 1) * block;
+  constexpr unsigned block = TMA_TILE;  // R_rows * nx: a compile-time stride for the stage layout
+  constexpr unsigned stage_elems = (M::Q + 1) * block;
   const int ntiles = nz * (ny / R_rows);
   const int rows_per_plane = ny / R_rows;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -204,11 +205,12 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       return;
     }
     const unsigned short* st = stages + s * stage_elems;
+    const unsigned short* mine = st + r * nx;  // this thread's row in population block 0
     const int z = t / rows_per_plane, y = (t % rows_per_plane) * R_rows + r;
     float2 v[M::Q];
 #pragma unroll
     for (int i = 0; i < M::Q; i++) {
-      const unsigned short* row = st + (size_t)i * block + r * nx;
+      const unsigned short* row = mine + i * block;  // constant offset per population
       if (M::ex(i) == 0) {
         v[i] = P16::unpack(*reinterpret_cast<const unsigned*>(row + x));
       } else if (M::ex(i) > 0) {  // from x-1
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
         v[i] = make_float2(P16::lo(row[x + 1]), P16::lo(row[xp2]));
       }
     }
-    const unsigned fl2 = *reinterpret_cast<const unsigned*>(st + (size_t)M::Q * block + r * nx + x);
+    const unsigned fl2 = *reinterpret_cast<const unsigned*>(mine + M::Q * block + x);
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&empty[s]));  // this warp is done with the stage
     const unsigned node = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)ny * (unsigned)z);

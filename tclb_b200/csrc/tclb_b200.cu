@@ -349,7 +349,7 @@ void setup_tma(tclb_lattice* L) {
   // Tiles of 512 nodes (R whole rows). Longer rows take the register pair
   // kernel: one-row tiles copied in two boxes measured slower than it.
   if (L->elem != 2 || L->nx % 64 || L->nx > 256) return;
-  const int R = 512 / L->nx;
+  const int R = (int)TMA_TILE / L->nx;
   if (L->ny % R) return;
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return;
