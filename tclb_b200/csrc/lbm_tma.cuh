@@ -195,18 +195,21 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   const int half = nx >> 1;
   const int r = tid / half, x = 2 * (tid % half);  // whole warps per row (nx >= 64)
   const int xm = x == 0 ? nx - 1 : x - 1, xp2 = x + 2 == nx ? 0 : x + 2;
-  for (int k = 0;; k++) {
-    const int t = blockIdx.x + k * gridDim.x;
-    if (t >= ntiles) break;
-    const int s = k % TMA_STAGES;
-    const bool ok = mbar_wait(smem_u32(&full[s]), (unsigned)(k / TMA_STAGES) & 1u);
+  // tile t = (z, yt) with yt = t mod rows_per_plane, stepped by gridDim.x per
+  // round without a division; the stage index and its phase likewise
+  const int dz = (int)gridDim.x / rows_per_plane, dyt = (int)gridDim.x % rows_per_plane;
+  int z = (int)blockIdx.x / rows_per_plane, yt = (int)blockIdx.x % rows_per_plane;
+  int s = 0;
+  unsigned phase = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const bool ok = mbar_wait(smem_u32(&full[s]), phase);
     if (!__all_sync(0xffffffffu, ok)) {  // the warp leaves together
       if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
       return;
     }
     const unsigned short* st = stages + s * stage_elems;
     const unsigned short* mine = st + r * nx;  // this thread's row in population block 0
-    const int z = t / rows_per_plane, y = (t % rows_per_plane) * R_rows + r;
+    const int y = yt * R_rows + r;
     float2 v[M::Q];
 #pragma unroll
     for (int i = 0; i < M::Q; i++) {
@@ -223,6 +226,16 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&empty[s]));  // this warp is done with the stage
     const unsigned node = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)ny * (unsigned)z);
+    if (++s == TMA_STAGES) {
+      s = 0;
+      phase ^= 1u;
+    }
+    z += dz;
+    yt += dyt;
+    if (yt >= rows_per_plane) {
+      yt -= rows_per_plane;
+      z++;
+    }
     pair_update_store<M, R, St>(v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
   }
 }
