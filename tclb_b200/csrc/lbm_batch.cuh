@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
 // One block per tile (grid = tile-table capacity; blocks past the live tiles
 // return at once): blocks are independent, as in the one-lattice kernel.
 template <class M, class R, class St, bool G>
-__global__ void __launch_bounds__(256) k_iterate_batch_tile(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(256, (G || sizeof(R) == 8) ? 1 : M::BATCH_MIN_BLOCKS)
+    k_iterate_batch_tile(const BatchCase* __restrict__ cases,
                                                             const BatchTile* __restrict__ tiles,
                                                             const int* __restrict__ ntiles_p, int k, int K) {
   const int t = blockIdx.x;

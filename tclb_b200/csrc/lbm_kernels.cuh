@@ -112,6 +112,7 @@ struct D2Q9 {
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
   static constexpr bool has_bulk = false;  // no packed two-node collision
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 1;
+  static constexpr int BATCH_MIN_BLOCKS = 6;  // one-tile batch kernel: <= 40 registers
   __device__ __forceinline__ static bool collides(flag_t) { return false; }
   __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
   template <class R>
@@ -290,6 +291,7 @@ struct D3Q19 {
   static constexpr bool has_bulk = true;
   // two-node kernel: 256 threads, <= 80 registers (3 blocks per SM), no spills
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 3;
+  static constexpr int BATCH_MIN_BLOCKS = 5;  // one-tile batch kernel: <= 48 registers
   // gamma1 = 1 - omega and gamma2 = 1 - 8(2 - omega)/(8 - omega), once per launch
   template <class R>
   __host__ __device__ static void derived(const R* s, R* k) {
@@ -591,6 +593,7 @@ struct D3Q27C {
   static constexpr bool has_bulk = true;
   // two-node kernel: 128 threads, <= 96 registers (5 blocks per SM), no spills
   static constexpr int PAIR_THREADS = 128, PAIR_MIN_BLOCKS = 5;
+  static constexpr int BATCH_MIN_BLOCKS = 4;  // one-tile batch kernel: <= 64 registers
   // relaxation rates of the bulk (nu) and of BOUNDARY nodes (nubuffer), once per launch
   template <class R>
   __host__ __device__ static void derived(const R* s, R* k) {
