@@ -2,9 +2,10 @@
 autotuner that picks their launch shape.
 
 A batch holds cases of one model/precision/storage; each ``step()`` enqueues
-one CUDA-graph replay that advances every active case by up to K iterations
-in one persistent launch per iteration. No counterpart in the reference (TCLB
-runs one lattice per process).
+one CUDA-graph replay that advances every active case by up to K iterations,
+one launch per iteration for all cases (one thread block per tile by
+default). No counterpart in the reference (TCLB runs one lattice per
+process).
 """
 from __future__ import annotations
 

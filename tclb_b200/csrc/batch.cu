@@ -1,6 +1,6 @@
-// Batched lattices: many independent cases of one model in one persistent,
-// graph-captured launch. New API (no counterpart in the reference, which runs
-// one lattice per process).
+// Batched lattices: many independent cases of one model advanced by one
+// launch per iteration, K iterations per CUDA-graph replay. New API (no
+// counterpart in the reference, which runs one lattice per process).
 //
 // Memory: each case is one allocation from a stream-ordered CUDA memory pool
 // owned by the batch (two snapshots, node types, zonal settings, Globals), so

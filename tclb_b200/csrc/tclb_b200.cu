@@ -239,7 +239,7 @@ struct Launch {
       else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
     }
   }
-  // Once at creation: shared-memory opt-in and persistent grid of the
+  // Once at creation: the dynamic shared-memory limit and persistent grid of the
   // tile-staged kernel (resident blocks per SM x SMs, at most one per tile).
   static void prepare(tclb_lattice* L) {
     using T = typename St::T;
