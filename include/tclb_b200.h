@@ -238,10 +238,12 @@ int tclb_batch_add_case(tclb_batch_h b, int nx, int ny, int nz, const uint16_t* 
 /* Retire a case and return its memory to the batch's pool (stream-ordered). */
 int tclb_batch_remove_case(tclb_batch_h b, int case_id);
 
-/* Launch shape: tile bx x by nodes per block (bx multiple of 32, bx*by <= 256),
-   iterations per replay, and grid: 0 (default) = one block per tile, > 0 = a
-   persistent grid of that many blocks walking the tiles, < 0 = persistent with
-   SMs x resident blocks. One block per tile measured fastest on mixed sizes. */
+/* Launch shape: tiles of bx x by nodes (bx a multiple of 32 up to 256, by up
+   to 256), iterations per replay, and grid: 0 (default) = one block per tile,
+   > 0 = a persistent grid of that many blocks walking the tiles, < 0 =
+   persistent with SMs x resident blocks. A block has bx x min(by, 256 / bx)
+   threads and walks the tile's rows. One block per tile measured fastest on
+   mixed sizes. */
 int tclb_batch_set_launch(tclb_batch_h b, int bx, int by, int iters_per_launch, int grid_blocks);
 /* Run the batch's work on a high-priority stream (high != 0) or a normal one:
    with batches of different models running at once, the blocks of the
@@ -249,6 +251,19 @@ int tclb_batch_set_launch(tclb_batch_h b, int bx, int by, int iters_per_launch, 
    wait behind large ones). Waits for the batch's work in flight. */
 int tclb_batch_set_priority(tclb_batch_h b, int high);
 int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launch);
+/* Paths of the plain launches: TCLB_LAUNCH_PAIRS (on by default) lets 16-bit
+   storage update two neighbouring nodes per thread with 32-bit accesses when
+   the tile width bx is a multiple of 64 and the grid is one block per tile
+   (blocks of bx / 2 x min(by, T / (bx / 2)) threads, T = 256, 128 for
+   d3q27_cumulant); the Globals launch keeps the one-node kernel.
+   TCLB_BATCH_SHORT_TILES (on by default) halves the tile height, down to the
+   block's thread rows, while the live cases would give fewer tiles than two
+   waves of resident blocks; off, tiles are always by rows high. get_paths
+   gives the flags that are enabled and apply to the current launch shape.
+   No TCLB counterpart. */
+#define TCLB_BATCH_SHORT_TILES 8
+int tclb_batch_set_paths(tclb_batch_h b, int flags);
+int tclb_batch_get_paths(tclb_batch_h b, int* flags);
 
 /* Enqueue one replay (asynchronous); every active case advances by
    min(iters_per_launch, remaining) iterations; Globals are those of each case's

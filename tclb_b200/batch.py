@@ -42,6 +42,8 @@ def _lib():
         L.tclb_batch_sync.argtypes = [h]
         L.tclb_batch_done.argtypes = [h]
         L.tclb_batch_set_priority.argtypes = [h, i]
+        L.tclb_batch_set_paths.argtypes = [h, i]
+        L.tclb_batch_get_paths.argtypes = [h, ip]
         L.tclb_batch_poll.argtypes = [h, i, ctypes.POINTER(ctypes.c_longlong), ip]
         L.tclb_batch_get_globals.argtypes = [h, i, dp]
         L.tclb_batch_get_quantity.argtypes = [h, i, i, vp, d]
@@ -155,6 +157,20 @@ class Batch:
         _check(self.lib.tclb_batch_get_launch(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
+    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True):
+        """use_pairs: 16-bit storage lets plain launches update two nodes per
+        thread when the tile shape allows it. short_tiles: lower the tile
+        height while the live cases give too few tiles to fill the GPU.
+        Both on by default."""
+        _check(self.lib.tclb_batch_set_paths(self._h, (2 if use_pairs else 0) | (8 if short_tiles else 0)))
+
+    def uses_pairs(self) -> bool:
+        """True when the plain launches of the current shape take the
+        two-nodes-per-thread kernel."""
+        f = ctypes.c_int()
+        _check(self.lib.tclb_batch_get_paths(self._h, ctypes.byref(f)))
+        return bool(f.value & 2)
+
     def step(self):
         _check(self.lib.tclb_batch_step(self._h))
 
@@ -212,7 +228,8 @@ class Batch:
 # ---------------------------------------------------------------------------
 # Autotuner
 # ---------------------------------------------------------------------------
-TILE_CANDIDATES = [(32, 8), (64, 4), (128, 2), (256, 1)]
+# tiles bx x by nodes; a block has at most 256 threads and walks taller tiles
+TILE_CANDIDATES = [(32, 8), (32, 32), (32, 64), (64, 16), (64, 64), (128, 16), (256, 8)]
 K_CANDIDATES = [1, 4, 16, 64]
 
 

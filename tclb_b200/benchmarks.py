@@ -234,7 +234,7 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150)
     for st in storages:
         reqs = serve_requests(n_requests, rate)
         srv = Server(("d2q9", "d3q19"), "fp32", st, budget_bytes=budget_gb << 30,
-                     launch={"d2q9": (128, 2, 64), "d3q19": (64, 4, 16)})
+                     launch={"d2q9": (64, 64, 64), "d3q19": (64, 16, 16) if st == "same" else (64, 64, 16)})
         rep = srv.run(reqs)
         done = srv.done
         srv.close()

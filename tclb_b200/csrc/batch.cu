@@ -37,16 +37,28 @@ int bfail(int code, const std::string& msg) {
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Kernel forms of the iteration launches.
+enum BatchForm { FORM_PERSISTENT = 0, FORM_TILE = 1, FORM_PAIR = 2 };
+
 struct BatchImpl {
-  void (*iterate)(const BatchCase*, const BatchTile*, const int*, int, int, dim3, dim3, bool, cudaStream_t);
+  // launch k of K over tiles of bx x by nodes; FORM_PAIR runs the pair kernel
+  // on plain launches (bx / 2 threads per row) and the one-tile kernel on the
+  // Globals launch (bx threads per row)
+  void (*iterate)(const BatchCase*, const BatchTile*, const int*, int, int, dim3, int bx, int by, int form,
+                  cudaStream_t);
   void (*clear)(BatchCase*, int, cudaStream_t);
   void (*init)(const BatchCase&, const void* dst, cudaStream_t, int bx, int by);
   void (*quantity)(const BatchCase&, int parity, int q, int vec, double scale, void* out, cudaStream_t);
   int (*blocks_per_sm)(int threads);
-  const void* (*tile_kernel)(bool globals);
+  const void* (*tile_kernel)(int which);  // 0 one-tile plain, 1 one-tile Globals, 2 pair
+  int pair_threads;                        // block-size limit of the pair kernel; 0: no pair kernel
   size_t real_size;
   int Q, NG, NSET, NZS, zone_shift;
 };
+
+// Thread rows of a block for tiles bx x by nodes with at most max_threads
+// threads: the block walks the remaining rows.
+int block_rows(int bx, int by, int max_threads) { return std::max(1, std::min(by, max_threads / bx)); }
 
 template <class M, class R>
 Args<R, M::NSET> args_of(const BatchCase& C, const void* src, void* dst) {
@@ -68,9 +80,18 @@ Args<R, M::NSET> args_of(const BatchCase& C, const void* src, void* dst) {
 template <class M, class R, class St>
 struct BL {
   // launch K-1 of a replay is every case's last iteration: the Globals variant
-  static void iterate(const BatchCase* c, const BatchTile* t, const int* n, int k, int K, dim3 g, dim3 b,
-                      bool per_tile, cudaStream_t s) {
-    if (per_tile) {
+  static constexpr bool pairs = sizeof(typename St::T) == 2;  // 16-bit storage
+  static void iterate(const BatchCase* c, const BatchTile* t, const int* n, int k, int K, dim3 g, int bx, int by,
+                      int form, cudaStream_t s) {
+    const dim3 b(bx, block_rows(bx, by, 256));
+    if constexpr (pairs) {
+      if (form == FORM_PAIR && k != K - 1) {
+        const dim3 bp(bx / 2, block_rows(bx / 2, by, M::PAIR_THREADS));
+        k_iterate_batch_pair<M, R, St><<<g, bp, 0, s>>>(c, t, n, k, K);
+        return;
+      }
+    }
+    if (form != FORM_PERSISTENT) {
       if (k == K - 1) k_iterate_batch_tile<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
       else k_iterate_batch_tile<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
     } else {
@@ -78,9 +99,13 @@ struct BL {
       else k_iterate_batch<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
     }
   }
-  static const void* tile_kernel(bool globals) {
-    return globals ? reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, true>)
-                   : reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, false>);
+  static const void* tile_kernel(int which) {
+    if constexpr (pairs) {
+      if (which == 2) return reinterpret_cast<const void*>(k_iterate_batch_pair<M, R, St>);
+    }
+    if (which == 2) return nullptr;
+    return which ? reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, true>)
+                 : reinterpret_cast<const void*>(k_iterate_batch_tile<M, R, St, false>);
   }
   // resident blocks per SM of the plain kernel at this block size
   static int blocks_per_sm(int threads) {
@@ -107,8 +132,9 @@ struct BL {
                                                       static_cast<R*>(out));
   }
   static const BatchImpl* get() {
-    static const BatchImpl impl = {iterate, clear, init, quantity, blocks_per_sm, tile_kernel, sizeof(R), M::Q,
-                                   M::NG, M::NSET, M::NZS, M::ZONE_SHIFT};
+    static const BatchImpl impl = {iterate,     clear, init, quantity, blocks_per_sm, tile_kernel,
+                                   pairs ? M::PAIR_THREADS : 0, sizeof(R), M::Q, M::NG, M::NSET, M::NZS,
+                                   M::ZONE_SHIFT};
     return &impl;
   }
 };
@@ -181,11 +207,14 @@ struct tclb_batch {
   bool tiles_dirty = true;
   int ntiles = 0;
   int bx = 128, by = 2, K = 16, grid_blocks = 0, user_grid = 0;
+  int sms = 148;   // multiprocessors of the device
+  int tile_h = 0;  // height of the tiles in the table
   cudaGraphExec_t graph = nullptr;
   cudaGraph_t graph_src = nullptr;            // kept: its nodes address the instantiated graph
   std::vector<cudaGraphNode_t> iter_nodes;    // the K iteration launches (one block per tile)
   int graph_grid = 0;                         // their grid size in the instantiated graph
-  int graph_key[5] = {-1, -1, -1, -1, -1};
+  int graph_key[6] = {-1, -1, -1, -1, -1, -1};
+  int paths = TCLB_LAUNCH_PAIRS | TCLB_BATCH_SHORT_TILES;  // tclb_batch_set_paths
 };
 
 namespace {
@@ -195,15 +224,49 @@ int upload_case(tclb_batch* B, int slot) {
   return TCLB_OK;
 }
 
+// Plain launches take the pair kernel: 16-bit storage, pairs enabled, one
+// block per tile, tile width a multiple of 64 and the block (bx / 2, by)
+// within the pair kernel's launch bounds.
+bool pair_form(const tclb_batch* B) {
+  return (B->paths & TCLB_LAUNCH_PAIRS) && B->user_grid == 0 && B->I->pair_threads > 0 && B->bx % 64 == 0 &&
+         B->bx / 2 <= B->I->pair_threads;
+}
+
+// Tile height: the set by, halved (down to the block's thread rows) while
+// the live cases would give fewer tiles than two waves of resident blocks --
+// a few small cases alone run as many short tiles, not a few long ones.
+int tile_height(const tclb_batch* B) {
+  int floor_h = block_rows(B->bx, B->by, 256);
+  if (pair_form(B)) floor_h = std::max(floor_h, block_rows(B->bx / 2, B->by, B->I->pair_threads));
+  if (!(B->paths & TCLB_BATCH_SHORT_TILES)) return B->by;
+  int per_sm = B->I->blocks_per_sm(B->bx * floor_h);
+  if (per_sm < 1) per_sm = std::max(1, 2048 / (B->bx * floor_h));
+  const size_t want = (size_t)2 * B->sms * per_sm;
+  auto count = [&](int h) {
+    size_t n = 0;
+    for (size_t s = 0; s < B->cases.size(); s++) {
+      const BatchCase& C = B->cases[s];
+      if (!B->used_slot[s] || !C.active || B->h_status[s].y <= 0) continue;
+      n += (size_t)C.nz * ((C.ny + h - 1) / h) * ((C.nx + B->bx - 1) / B->bx);
+    }
+    return n;
+  };
+  int h = B->by;
+  while (h > floor_h && count(h) < want) h = std::max(floor_h, h / 2);
+  return h;
+}
+
 int rebuild_tiles(tclb_batch* B) {
   std::vector<BatchTile> t;
+  const int h = tile_height(B);
   for (size_t s = 0; s < B->cases.size(); s++) {
     const BatchCase& C = B->cases[s];
     if (!B->used_slot[s] || !C.active || B->h_status[s].y <= 0) continue;  // finished cases get no tiles
     for (int z = 0; z < C.nz; z++)
-      for (int y = 0; y < C.ny; y += B->by)
-        for (int x = 0; x < C.nx; x += B->bx) t.push_back({(int)s, x, y, z});
+      for (int y = 0; y < C.ny; y += h)
+        for (int x = 0; x < C.nx; x += B->bx) t.push_back({(int)s, x, y, z, h});
   }
+  B->tile_h = h;
   if (t.size() > B->tiles_cap) {
     if (B->d_tiles) BCK(cudaFreeAsync(B->d_tiles, B->stream));
     B->tiles_cap = std::max(t.size(), B->tiles_cap * 2);
@@ -236,8 +299,8 @@ int update_graph_grid(tclb_batch* B) {
 }
 
 int ensure_graph(tclb_batch* B) {
-  const int key[5] = {B->bx, B->by, B->K, (int)B->cases.size(), B->user_grid};
-  if (B->graph && std::equal(key, key + 5, B->graph_key)) return update_graph_grid(B);
+  const int key[6] = {B->bx, B->by, B->K, (int)B->cases.size(), B->user_grid, B->paths};
+  if (B->graph && std::equal(key, key + 6, B->graph_key)) return update_graph_grid(B);
   if (B->graph) {
     cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
@@ -249,19 +312,21 @@ int ensure_graph(tclb_batch* B) {
   B->iter_nodes.clear();
   int dev = B->device, sms = 148, per_sm = 4;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  per_sm = B->I->blocks_per_sm(B->bx * B->by);
-  if (per_sm < 1) per_sm = std::max(1, 2048 / (B->bx * B->by));
+  const int threads = B->bx * block_rows(B->bx, B->by, 256);
+  per_sm = B->I->blocks_per_sm(threads);
+  if (per_sm < 1) per_sm = std::max(1, 2048 / threads);
   // grid_blocks 0 (default): one block per live tile; > 0: a persistent grid
   // of that size walking the tiles; < 0: persistent, SMs x resident blocks.
   const bool per_tile = B->user_grid == 0;
   B->grid_blocks = per_tile ? std::max(1, B->ntiles) : (B->user_grid > 0 ? B->user_grid : sms * per_sm);
+  const int form = !per_tile ? FORM_PERSISTENT : (pair_form(B) ? FORM_PAIR : FORM_TILE);
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   const int n = (int)B->cases.size();
   B->I->clear(B->d_cases, n, B->stream);
   for (int k = 0; k < B->K; k++)
-    B->I->iterate(B->d_cases, B->d_tiles, B->d_ntiles, k, B->K, dim3(B->grid_blocks), dim3(B->bx, B->by),
-                  per_tile, B->stream);
+    B->I->iterate(B->d_cases, B->d_tiles, B->d_ntiles, k, B->K, dim3(B->grid_blocks), B->bx, B->by, form,
+                  B->stream);
   if (n > 0) {
     k_batch_advance<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->K);
     k_batch_status<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->d_status);
@@ -279,19 +344,20 @@ int ensure_graph(tclb_batch* B) {
     BCK(cudaGraphGetNodes(g, nullptr, &count));
     std::vector<cudaGraphNode_t> nodes(count);
     BCK(cudaGraphGetNodes(g, nodes.data(), &count));
-    const void* f0 = B->I->tile_kernel(false);
-    const void* f1 = B->I->tile_kernel(true);
+    const void* f0 = B->I->tile_kernel(0);
+    const void* f1 = B->I->tile_kernel(1);
+    const void* f2 = B->I->tile_kernel(2);
     for (cudaGraphNode_t node : nodes) {
       cudaGraphNodeType type;
       BCK(cudaGraphNodeGetType(node, &type));
       if (type != cudaGraphNodeTypeKernel) continue;
       cudaKernelNodeParams p;
       BCK(cudaGraphKernelNodeGetParams(node, &p));
-      if (p.func == f0 || p.func == f1) B->iter_nodes.push_back(node);
+      if (p.func == f0 || p.func == f1 || (f2 && p.func == f2)) B->iter_nodes.push_back(node);
     }
   }
   B->graph_grid = B->grid_blocks;
-  std::copy(key, key + 5, B->graph_key);
+  std::copy(key, key + 6, B->graph_key);
   return TCLB_OK;
 }
 
@@ -325,6 +391,7 @@ int tclb_batch_create(tclb_batch_h* out, int model, int precision, int storage, 
   B->budget = budget_bytes;
   B->max_cases = max_cases;
   cudaGetDevice(&B->device);
+  cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, B->device);
   cudaMemPoolProps props = {};
   props.allocType = cudaMemAllocationTypePinned;
   props.location.type = cudaMemLocationTypeDevice;
@@ -468,7 +535,7 @@ int tclb_batch_set_priority(tclb_batch_h B, int high) {
 
 int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, int grid_blocks) {
   CHECK_B(B);
-  if (bx < 32 || bx % 32 || by < 1 || bx * by > 256 || iters_per_launch < 1 || iters_per_launch > 4096)
+  if (bx < 32 || bx % 32 || bx > 256 || by < 1 || by > 256 || iters_per_launch < 1 || iters_per_launch > 4096)
     return bfail(TCLB_ERR_ARG, "bad launch shape");
   if (bx != B->bx || by != B->by) B->tiles_dirty = true;
   B->bx = bx;
@@ -476,6 +543,21 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
   B->K = iters_per_launch;
   B->user_grid = grid_blocks;
   B->graph_key[0] = -1;
+  return TCLB_OK;
+}
+
+int tclb_batch_set_paths(tclb_batch_h B, int flags) {
+  CHECK_B(B);
+  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_BATCH_SHORT_TILES)) return bfail(TCLB_ERR_ARG, "unknown path flags");
+  if ((flags ^ B->paths) & TCLB_BATCH_SHORT_TILES) B->tiles_dirty = true;
+  B->paths = flags;
+  B->graph_key[0] = -1;
+  return TCLB_OK;
+}
+
+int tclb_batch_get_paths(tclb_batch_h B, int* flags) {
+  CHECK_B(B);
+  if (flags) *flags = (pair_form(B) ? TCLB_LAUNCH_PAIRS : 0) | (B->paths & TCLB_BATCH_SHORT_TILES);
   return TCLB_OK;
 }
 

@@ -12,7 +12,11 @@
 //
 // A tile is a bx x by block of nodes of one z plane of one case. With nx a
 // multiple of 32 (TCLB's padding) a tile width of 32 leaves no thread idle on
-// any case; wider tiles trade that for fewer tiles. The autotuner chooses.
+// any case; wider tiles trade that for fewer tiles. A thread block has at
+// most 256 threads (bx x min(by, 256 / bx)) and walks the tile's rows, so a
+// taller tile spreads the block's descriptor reads over more nodes. The
+// autotuner chooses the shape; the tile table lowers the height when the live
+// cases would give too few tiles to fill the GPU.
 //
 // A launch is iteration k (0-based) of a replay of K iterations. A case with
 // d = min(remaining, K) iterations to do in this replay runs the last d
@@ -45,6 +49,7 @@ struct BatchCase {
 
 struct BatchTile {
   int slot, x0, y0, z;
+  int h;  // rows: the tile is bx x h nodes
 };
 
 template <class M, class R, class St, bool G>
@@ -85,44 +90,41 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
         M::template derived<R>(a.s, a.k);
       }
       if (skip) continue;
-      const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
-      const bool act = x < a.nx && y < a.ny;
+      const int x = tile.x0 + threadIdx.x, z = tile.z;
+      const int y_end = min(tile.y0 + tile.h, a.ny);
       using T = typename St::T;
       const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
       if constexpr (G) {
         R g[M::NG];
 #pragma unroll
         for (int i = 0; i < M::NG; i++) g[i] = 0;
-        if (act) node_update<M, R, St, true>(a, P, x, y, z, g);
+        if (x < a.nx)
+          for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y) node_update<M, R, St, true>(a, P, x, y, z, g);
         reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
         __syncthreads();  // shared scratch of reduce_globals reused by the next tile
-      } else {
-        if (act) {
-          R g[1];
-          node_update<M, R, St, false>(a, P, x, y, z, g);
-        }
+      } else if (x < a.nx) {
+        R g[1];
+        for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y) node_update<M, R, St, false>(a, P, x, y, z, g);
       }
     }
   }
 }
 
-// One block per tile (grid = tile-table capacity; blocks past the live tiles
-// return at once): blocks are independent, as in the one-lattice kernel.
-template <class M, class R, class St, bool G>
-__global__ void __launch_bounds__(256, (G || sizeof(R) == 8) ? 1 : M::BATCH_MIN_BLOCKS)
-    k_iterate_batch_tile(const BatchCase* __restrict__ cases,
-                                                            const BatchTile* __restrict__ tiles,
-                                                            const int* __restrict__ ntiles_p, int k, int K) {
+// The arguments of tile t at launch k of a replay of K; false if the block
+// has nothing to do (past the live tiles, or the case idle at this launch).
+template <class M, class R>
+__device__ __forceinline__ bool batch_tile_args(const BatchCase* __restrict__ cases,
+                                                const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles_p,
+                                                int k, int K, BatchTile& tile, Args<R, M::NSET>& a) {
   const int t = blockIdx.x;
-  if (t >= *ntiles_p) return;
-  const BatchTile tile = tiles[t];
+  if (t >= *ntiles_p) return false;
+  tile = tiles[t];
   const BatchCase& C = cases[tile.slot];
   const int remaining = C.remaining;
   const int d = remaining < K ? remaining : K;
   const int first = K - d;
-  if (!C.active || d <= 0 || k < first) return;
+  if (!C.active || d <= 0 || k < first) return false;
   const int parity = (C.counter + (k - first)) & 1;
-  Args<R, M::NSET> a;
   a.src = C.buf[parity];
   a.dst = C.buf[1 - parity];
   a.stride = C.stride;
@@ -135,20 +137,65 @@ __global__ void __launch_bounds__(256, (G || sizeof(R) == 8) ? 1 : M::BATCH_MIN_
 #pragma unroll
   for (int i = 0; i < M::NSET; i++) a.s[i] = (R)C.s[i];
   M::template derived<R>(a.s, a.k);
-  const int x = tile.x0 + threadIdx.x, y = tile.y0 + threadIdx.y, z = tile.z;
-  const bool act = x < a.nx && y < a.ny;
+  return true;
+}
+
+// One block per tile (grid = live tiles): blocks are independent, as in the
+// one-lattice kernel. A block of bx x by threads walks the tile's h rows with
+// stride by, so its descriptor reads are spread over h / by nodes per thread.
+template <class M, class R, class St, bool G>
+__global__ void __launch_bounds__(256, (G || sizeof(R) == 8) ? 1 : M::BATCH_MIN_BLOCKS)
+    k_iterate_batch_tile(const BatchCase* __restrict__ cases, const BatchTile* __restrict__ tiles,
+                         const int* __restrict__ ntiles_p, int k, int K) {
+  BatchTile tile;
+  Args<R, M::NSET> a;
+  if (!batch_tile_args<M, R>(cases, tiles, ntiles_p, k, K, tile, a)) return;
+  const int x = tile.x0 + threadIdx.x, z = tile.z;
+  const int y_end = min(tile.y0 + tile.h, a.ny);
   using T = typename St::T;
   const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
   if constexpr (G) {
     R g[M::NG];
 #pragma unroll
     for (int i = 0; i < M::NG; i++) g[i] = 0;
-    if (act) node_update<M, R, St, true>(a, P, x, y, z, g);
+    if (x < a.nx)
+      for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y) node_update<M, R, St, true>(a, P, x, y, z, g);
     reduce_globals<M::NG, M::NSUM, R>(g, a.glob);
-  } else if (act) {
+  } else if (x < a.nx) {
     R g[1];
-    node_update<M, R, St, false>(a, P, x, y, z, g);
+    for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y) node_update<M, R, St, false>(a, P, x, y, z, g);
   }
+}
+
+// 16-bit storage, plain launches: two neighbouring nodes per thread with
+// 32-bit accesses, the update of the one-lattice pair kernel. A tile of
+// bx x h nodes (bx a multiple of 64) runs as a block of bx / 2 x by threads
+// walking the rows with stride by; each warp covers 64 consecutive x of one
+// row. In the last tile of a row whose width is not a
+// multiple of 64 the lanes past the row only load (node_update_pair's
+// PARTIAL form). A case with odd nx has no node pairs: its tiles take the
+// one-node update, two nodes per thread.
+template <class M, class R, class St>
+__global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
+    k_iterate_batch_pair(const BatchCase* __restrict__ cases, const BatchTile* __restrict__ tiles,
+                         const int* __restrict__ ntiles_p, int k, int K) {
+  BatchTile tile;
+  Args<R, M::NSET> a;
+  if (!batch_tile_args<M, R>(cases, tiles, ntiles_p, k, K, tile, a)) return;
+  using T = typename St::T;
+  const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
+  const int z = tile.z;
+  const int y_end = min(tile.y0 + tile.h, a.ny);  // y is uniform per warp: a warp lies in one row
+  if (a.nx & 1) {
+    R g[1];
+    for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y)
+      for (int x = tile.x0 + threadIdx.x; x < tile.x0 + 2 * (int)blockDim.x && x < a.nx; x += blockDim.x)
+        node_update<M, R, St, false>(a, P, x, y, z, g);
+    return;
+  }
+  const int x = tile.x0 + 2 * threadIdx.x;
+  for (int y = tile.y0 + threadIdx.y; y < y_end; y += blockDim.y)
+    node_update_pair<M, R, St, StrideAddr<T>, true>(a, P, x, y, z, threadIdx.x & 31);
 }
 
 // End of a replay: counters and remaining iterations of every active case.

@@ -111,7 +111,7 @@ struct D2Q9 {
   static constexpr int Q = 9, DIM = 2, NSET = d2q9::NSET, NZS = d2q9::NZS, NG = d2q9::NG, NSUM = d2q9::NSUM,
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
   static constexpr bool has_bulk = false;  // no packed two-node collision
-  static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 1;
+  static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 4;  // <= 64 registers
   static constexpr int BATCH_MIN_BLOCKS = 6;  // one-tile batch kernel: <= 40 registers
   __device__ __forceinline__ static bool collides(flag_t) { return false; }
   __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
@@ -1032,10 +1032,9 @@ struct Pack16<StoreBF16<SH>> {
 // Models with a packed collision: boundary conditions per node, then one
 // FP32x2 collision for both; others: the scalar node update twice. Plain
 // iterations (no Globals).
-template <class M, class R, class St>
+template <class M, class R, class St, class A>
 __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb,
-                                                  const Args<R, M::NSET>& a,
-                                                  const PlaneAddr<typename St::T, M::Q>& P, unsigned node) {
+                                                  const Args<R, M::NSET>& a, const A& P, unsigned node) {
   using P16 = Pack16<St>;
   if constexpr (M::has_bulk && sizeof(R) == 4) {
     // Values stay packed (node x, node x+1). A node with a boundary type has
@@ -1111,12 +1110,21 @@ __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla,
   }
 }
 
-template <class M, class R, class St>
-__device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a,
-                                                 const PlaneAddr<typename St::T, M::Q>& P, int x, int y, int z,
+// PARTIAL: x may lie past the row (the last tile of a row whose width is not
+// a multiple of 64); such a lane loads the pair at x mod nx, which its
+// neighbours' shuffles need, and stores nothing.
+template <class M, class R, class St, class A, bool PARTIAL = false>
+__device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a, const A& P, int x, int y, int z,
                                                  int lane) {
   using P16 = Pack16<St>;
   const unsigned nx = a.nx, ny = a.ny, nz = a.nz;
+  bool store = true;
+  if constexpr (PARTIAL) {
+    if (x >= a.nx) {
+      x = (unsigned)x % nx;
+      store = false;
+    }
+  }
   const unsigned sxy = nx * ny;
   const unsigned node = x + nx * y + sxy * z;  // even
   const unsigned oy_lo = y == 0 ? nx * (ny - 1) : 0u - nx, oy_hi = y + 1 == (int)ny ? nx * (1u - ny) : nx;
@@ -1145,7 +1153,7 @@ __device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a,
       v[i] = make_float2(P16::hi(w), P16::lo(next));
     }
   }
-  pair_update_store<M, R, St>(v, fla, flb, a, P, node);
+  if (!PARTIAL || store) pair_update_store<M, R, St>(v, fla, flb, a, P, node);
 }
 
 // Block (32, M::PAIR_THREADS / 32): each warp covers 64 consecutive x of one
@@ -1157,7 +1165,7 @@ __global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
   const int x = 2 * (blockIdx.x * 32 + lane);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
-  if (y < a.ny) node_update_pair<M, R, St>(a, P, x, y, z, lane);  // y is uniform per warp
+  if (y < a.ny) node_update_pair<M, R, St, PlaneAddr<typename St::T, M::Q>>(a, P, x, y, z, lane);  // y is uniform per warp
 }
 
 template <class M, class R, class St, bool G, class A>

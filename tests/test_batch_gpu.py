@@ -69,7 +69,7 @@ def test_result_same_alone_and_in_the_mix():
     alone.run_to_completion()
     u_alone = alone.quantity(a, "U")
     mix = Batch("d2q9", "fp32", storage="fp16s")
-    mix.set_launch(32, 8, 5)
+    mix.set_launch(64, 4, 5)  # another tile shape and K, the same (two-nodes-per-thread) kernel form
     ids = [mix.add_case(s) for s in specs]
     mix.run_to_completion()
     u_mix = mix.quantity(ids[1], "U")
@@ -120,3 +120,145 @@ def test_autotune_picks_a_valid_shape():
     r = autotune("d2q9", specs, tiles=[(32, 8), (128, 2)], ks=[1, 8], trial_iters=16)
     assert (r["bx"], r["by"]) in [(32, 8), (128, 2)] and r["K"] in (1, 8)
     assert r["mlups"] > 0 and len(r["table"]) == 4
+
+
+def test_batch_pair_paths_apply():
+    """16-bit storage takes the two-nodes-per-thread kernel on plain launches
+    when the tile width is a multiple of 64 and the block fits; FP32 never."""
+    b = Batch("d3q27_cumulant", "fp32", storage="fp16s", budget_bytes=1 << 28)
+    for (bx, by), want in {(64, 4): True, (128, 2): True, (256, 1): True, (32, 8): False}.items():
+        b.set_launch(bx, by, 4)
+        assert b.uses_pairs() == want, (bx, by)
+    b.set_launch(64, 4, 4)
+    b.set_paths(use_pairs=False)
+    assert not b.uses_pairs()
+    b.close()
+    b = Batch("d2q9", "fp32", budget_bytes=1 << 28)
+    b.set_launch(128, 2, 4)
+    assert not b.uses_pairs()
+    b.close()
+
+
+def _doubled(spec):
+    """The case twice side by side in x: with periodic wrap every node of the
+    doubled lattice sees the same neighbourhood as in the case itself."""
+    return CaseSpec(np.concatenate([spec.flags, spec.flags], axis=-1), spec.settings, spec.zone_settings, spec.niter)
+
+
+def _random_case(model, shape, seed, niter=6):
+    """Random node types of every boundary class, three zones, the parity
+    tests' settings: flow from the first iteration on."""
+    from helpers import random_flags
+    from test_parity_gpu import BOUNDARY_TYPES, EXTRA_GROUPS, PARAMS
+
+    fl = random_flags(model, shape, BOUNDARY_TYPES[model], zones=3, seed=seed, p_type=0.15,
+                      extra_groups=EXTRA_GROUPS[model])
+    settings = {p[1]: p[2] for p in PARAMS[model] if p[0] == "setting"}
+    zones = {}
+    for p in PARAMS[model]:
+        if p[0] == "zone":
+            zones.setdefault(p[3], {})[p[1]] = p[2]
+    return CaseSpec(fl, settings, zones, niter)
+
+
+PAIR_SHAPES = {"d2q9": [(1, 24, 96), (1, 16, 64)], "d3q19": [(6, 8, 96)], "d3q27_cumulant": [(4, 8, 160)]}
+
+
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+@pytest.mark.parametrize("storage", ["fp16s", "bf16"])
+def test_batch_pair_kernel_partial_tiles(model, storage):
+    """The batch's pair kernel on cases whose width is not a multiple of 64
+    (the last tile of each row is half past the row: those lanes load the
+    wrapped pair and store nothing) against the doubled case in the same
+    batch (no partial tile): bit for bit. Then against the single-lattice
+    pair kernel on the doubled case: the settings reach the two kernels by
+    different roundings, so a 16-bit rounding may flip (1e-3 relative L2)."""
+    specs = [_random_case(model, sh, seed=11 + i) for i, sh in enumerate(PAIR_SHAPES[model])]
+    b = Batch(model, "fp32", storage=storage, budget_bytes=1 << 30)
+    b.set_launch(64, 4, 4)
+    assert b.uses_pairs()
+    ids = [(b.add_case(s), b.add_case(_doubled(s))) for s in specs]
+    b.run_to_completion()
+    qs = (M.get(model).quantities[0][0], "U")
+    for (cid, did), s in zip(ids, specs):
+        half = s.shape[-1]
+        for q in qs:
+            got, dbl = b.quantity(cid, q), b.quantity(did, q)
+            if q == "U":
+                dbl = np.moveaxis(dbl, -1, 0)
+                got = np.moveaxis(got, -1, 0)
+            assert np.array_equal(got, dbl[..., :half]) and np.array_equal(got, dbl[..., half:]), q
+        d = _doubled(s)
+        nz, ny, nx = d.shape
+        lat = Lattice(model, nx, ny, nz, precision="fp32", storage=storage)
+        lat.set_launch(32, 8, use_tma=False)
+        assert lat.launch_path()["pairs"]
+        lat.set_flags(d.flags)
+        for k, v in d.settings.items():
+            lat.SetSetting(k, v)
+        for z, dd in d.zone_settings.items():
+            for k, v in dd.items():
+                lat.set_zone_setting(k, v, z)
+        lat.Init()
+        lat.Iterate(d.niter, M.ITER_NORM | M.ITER_LASTGLOB)
+        for q in qs:
+            assert rel_l2(b.quantity(did, q), lat.GetQuantity(q)) <= 1e-3, q
+        lat.close()
+    b.close()
+
+
+def test_batch_pair_kernel_odd_width_takes_one_node_update():
+    """A case with odd nx has no node pairs: in the pair form its tiles run the
+    one-node update; the result matches the batch's one-node form."""
+    fl = cases.disc_channel_flags(97, 32, 5.0, 24, 16)
+    spec = CaseSpec(fl, {"Viscosity": 0.03}, {0: {"VelocityX": 0.02}}, 12)
+    out = []
+    for bx, by in ((64, 4), (32, 8)):
+        b = Batch("d2q9", "fp32", storage="fp16s", budget_bytes=1 << 28)
+        b.set_launch(bx, by, 4)
+        c = b.add_case(spec)
+        b.run_to_completion()
+        out.append(b.quantity(c, "U"))
+        b.close()
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("storage,short,tall", [("same", (32, 8), (32, 48)), ("fp16s", (64, 4), (64, 24))])
+def test_tall_tiles_walk_rows(storage, short, tall):
+    """Tiles taller than the block (each thread walks several rows, the last
+    pass partly past the tile) give the same fields as short tiles, and the
+    same Globals up to summation order (a thread sums its rows in FP32
+    before the FP64 block reduction)."""
+    specs = [_random_case("d3q19", (5, 40, 64), seed=21, niter=7), _random_case("d3q19", (3, 13, 96), seed=22, niter=7)]
+    out = []
+    for bx, by in (short, tall):
+        b = Batch("d3q19", "fp32", storage=storage, budget_bytes=1 << 30)
+        b.set_launch(bx, by, 3)
+        b.set_paths(short_tiles=False)  # these few small cases would get short tiles
+        ids = [b.add_case(s) for s in specs]
+        b.step()
+        want = sum(s.shape[0] * -(-s.shape[1] // by) * -(-s.shape[2] // bx) for s in specs)
+        assert b.info()["tiles"] == want
+        b.run_to_completion()
+        out.append([(b.quantity(c, "U"), b.globals(c)) for c in ids])
+        b.close()
+    for (u0, g0), (u1, g1) in zip(*out):
+        assert np.array_equal(u0, u1)
+        assert np.allclose(g0, g1, rtol=1e-6, atol=1e-12)
+
+
+def test_short_tiles_when_few():
+    """With few live tiles the table lowers the tile height (more, shorter
+    tiles); the fields stay the same."""
+    spec = _random_case("d2q9", (1, 64, 128), seed=31, niter=5)
+    res = []
+    for short in (True, False):
+        b = Batch("d2q9", "fp32", budget_bytes=1 << 28)
+        b.set_launch(64, 64, 5)
+        b.set_paths(short_tiles=short)
+        c = b.add_case(spec)
+        b.step()
+        res.append((b.info()["tiles"], b.quantity(c, "U")))
+        b.close()
+    assert res[1][0] == 2 and res[0][0] == 2 * 64 // 4  # short: 4-row tiles (the block's thread rows)
+    assert np.array_equal(res[0][1], res[1][1])
