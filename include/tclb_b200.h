@@ -256,11 +256,16 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    the tile width bx is a multiple of 64 and the grid is one block per tile
    (blocks of bx / 2 x min(by, T / (bx / 2)) threads, T = 256, 128 for
    d3q27_cumulant); the Globals launch keeps the one-node kernel.
-   TCLB_BATCH_SHORT_TILES (on by default) halves the tile height, down to the
+   TCLB_LAUNCH_TMA (on by default) runs the plain launches of each 16-bit case
+   whose rows fit one TMA box (nx a multiple of 64 up to 256, 512 / nx
+   dividing ny) through the tile-staged kernel, tensor maps kept with the case;
+   the other cases take the pair or one-node form. A staging wait that runs
+   out (about a second) is reported as TCLB_ERR_CUDA by the next
+   tclb_batch_sync. TCLB_BATCH_SHORT_TILES (on by default) halves the tile height, down to the
    block's thread rows, while the live cases would give fewer tiles than two
    waves of resident blocks; off, tiles are always by rows high. get_paths
-   gives the flags that are enabled and apply to the current launch shape.
-   No TCLB counterpart. */
+   gives the flags that are enabled and apply to the current launch shape
+   (TCLB_LAUNCH_TMA: to at least one live case). No TCLB counterpart. */
 #define TCLB_BATCH_SHORT_TILES 8
 int tclb_batch_set_paths(tclb_batch_h b, int flags);
 int tclb_batch_get_paths(tclb_batch_h b, int* flags);

@@ -157,19 +157,28 @@ class Batch:
         _check(self.lib.tclb_batch_get_launch(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
-    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True):
+    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True, use_tma: bool = True):
         """use_pairs: 16-bit storage lets plain launches update two nodes per
         thread when the tile shape allows it. short_tiles: lower the tile
         height while the live cases give too few tiles to fill the GPU.
-        Both on by default."""
-        _check(self.lib.tclb_batch_set_paths(self._h, (2 if use_pairs else 0) | (8 if short_tiles else 0)))
+        use_tma: 16-bit cases whose rows fit one TMA box take the tile-staged
+        kernel. All on by default."""
+        flags = (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if short_tiles else 0)
+        _check(self.lib.tclb_batch_set_paths(self._h, flags))
+
+    def _paths(self) -> int:
+        f = ctypes.c_int()
+        _check(self.lib.tclb_batch_get_paths(self._h, ctypes.byref(f)))
+        return f.value
 
     def uses_pairs(self) -> bool:
         """True when the plain launches of the current shape take the
-        two-nodes-per-thread kernel."""
-        f = ctypes.c_int()
-        _check(self.lib.tclb_batch_get_paths(self._h, ctypes.byref(f)))
-        return bool(f.value & 2)
+        two-nodes-per-thread kernel (for the cases not tile-staged)."""
+        return bool(self._paths() & 2)
+
+    def uses_tma(self) -> bool:
+        """True when at least one live case takes the tile-staged kernel."""
+        return bool(self._paths() & 4)
 
     def step(self):
         _check(self.lib.tclb_batch_step(self._h))

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -40,18 +41,38 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Kernel forms of the iteration launches.
 enum BatchForm { FORM_PERSISTENT = 0, FORM_TILE = 1, FORM_PAIR = 2 };
 
+// The device tables a replay's launches read.
+struct LaunchTables {
+  const BatchCase* cases;
+  const BatchTile* tiles;      // tiles of the cases not staged, then those of the staged cases
+  const int* ntiles;           // [0] tiles of the cases not staged, [1] all tiles
+  const BatchTmaTile* ttiles;  // tiles of the tile-staged kernel
+  const int* nttiles;
+  int* err;                    // set by a staging wait that ran out
+};
+
 struct BatchImpl {
-  // launch k of K over tiles of bx x by nodes; FORM_PAIR runs the pair kernel
-  // on plain launches (bx / 2 threads per row) and the one-tile kernel on the
-  // Globals launch (bx threads per row)
-  void (*iterate)(const BatchCase*, const BatchTile*, const int*, int, int, dim3, int bx, int by, int form,
-                  cudaStream_t);
+  // Launch k of K. Plain launches: the tile-staged kernel over the staged
+  // cases when tma_grid > 0, then the plain form over the other cases' tiles
+  // (grid gp); FORM_PAIR takes the pair kernel (bx / 2 threads per row). The
+  // Globals launch (k = K-1): the one-tile kernel over every case's tiles
+  // (grid ga, bx threads per row).
+  // group: the settings shared by the staged cases (models with the packed
+  // collision; see tclb_batch::group)
+  void (*iterate)(const LaunchTables&, int k, int K, dim3 gp, dim3 ga, int tma_grid, const double* group, int bx,
+                  int by, int form, cudaStream_t);
+  // resident blocks of the tile-staged kernel on the device (it also sets the
+  // kernel's shared-memory limit); 0 without one
+  int (*tma_grid)(int sms);
+  // the derived constants k of a case from its settings (host, in real_t)
+  void (*derive)(BatchCase&);
   void (*clear)(BatchCase*, int, cudaStream_t);
   void (*init)(const BatchCase&, const void* dst, cudaStream_t, int bx, int by);
   void (*quantity)(const BatchCase&, int parity, int q, int vec, double scale, void* out, cudaStream_t);
   int (*blocks_per_sm)(int threads);
   const void* (*tile_kernel)(int which);  // 0 one-tile plain, 1 one-tile Globals, 2 pair
   int pair_threads;                        // block-size limit of the pair kernel; 0: no pair kernel
+  bool group_staging;                      // staged cases must share their settings (packed collision)
   size_t real_size;
   int Q, NG, NSET, NZS, zone_shift;
 };
@@ -81,23 +102,52 @@ template <class M, class R, class St>
 struct BL {
   // launch K-1 of a replay is every case's last iteration: the Globals variant
   static constexpr bool pairs = sizeof(typename St::T) == 2;  // 16-bit storage
-  static void iterate(const BatchCase* c, const BatchTile* t, const int* n, int k, int K, dim3 g, int bx, int by,
-                      int form, cudaStream_t s) {
+  static size_t tma_smem() { return 128 + (size_t)tma_stages<M>() * (M::Q + 1) * TMA_TILE * 2; }
+  static void iterate(const LaunchTables& L, int k, int K, dim3 gp, dim3 ga, int tma_grid, const double* group,
+                      int bx, int by, int form, cudaStream_t s) {
     const dim3 b(bx, block_rows(bx, by, 256));
+    const BatchCase* c = L.cases;
+    const BatchTile* t = L.tiles;
+    if (k == K - 1) {  // every case's last iteration of the replay: Globals, all tiles
+      if (form == FORM_PERSISTENT) k_iterate_batch<M, R, St, true><<<gp, b, 0, s>>>(c, t, L.ntiles + 1, k, K);
+      else k_iterate_batch_tile<M, R, St, true><<<ga, b, 0, s>>>(c, t, L.ntiles + 1, k, K);
+      return;
+    }
     if constexpr (pairs) {
-      if (form == FORM_PAIR && k != K - 1) {
+      if (tma_grid > 0) {
+        BatchCase G;  // the group's settings and derived constants
+        std::memset(&G, 0, sizeof(G));
+        if (group)
+          for (int i = 0; i < M::NSET; i++) G.s[i] = group[i];
+        const Args<R, M::NSET> gargs = args_of<M, R>(G, nullptr, nullptr);
+        k_iterate_batch_tma<M, R, St>
+            <<<tma_grid, TMA_THREADS, tma_smem(), s>>>(c, L.ttiles, L.nttiles, k, K, L.err, gargs);
+      }
+      if (form == FORM_PAIR) {
         const dim3 bp(bx / 2, block_rows(bx / 2, by, M::PAIR_THREADS));
-        k_iterate_batch_pair<M, R, St><<<g, bp, 0, s>>>(c, t, n, k, K);
+        k_iterate_batch_pair<M, R, St><<<gp, bp, 0, s>>>(c, t, L.ntiles, k, K);
         return;
       }
     }
-    if (form != FORM_PERSISTENT) {
-      if (k == K - 1) k_iterate_batch_tile<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
-      else k_iterate_batch_tile<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
-    } else {
-      if (k == K - 1) k_iterate_batch<M, R, St, true><<<g, b, 0, s>>>(c, t, n, k, K);
-      else k_iterate_batch<M, R, St, false><<<g, b, 0, s>>>(c, t, n, k, K);
+    if (form == FORM_PERSISTENT) k_iterate_batch<M, R, St, false><<<gp, b, 0, s>>>(c, t, L.ntiles, k, K);
+    else k_iterate_batch_tile<M, R, St, false><<<gp, b, 0, s>>>(c, t, L.ntiles, k, K);
+  }
+  static void derive(BatchCase& C) {
+    const Args<R, M::NSET> a = args_of<M, R>(C, nullptr, nullptr);
+    for (int i = 0; i < 4; i++) C.k[i] = (double)a.k[i];
+  }
+  static int tma_grid(int sms) {
+    if constexpr (pairs) {
+      const void* f = reinterpret_cast<const void*>(k_iterate_batch_tma<M, R, St>);
+      int n = 0;
+      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem()) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, TMA_THREADS, tma_smem()) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+      }
+      return n * sms;
     }
+    return 0;
   }
   static const void* tile_kernel(int which) {
     if constexpr (pairs) {
@@ -132,8 +182,21 @@ struct BL {
                                                       static_cast<R*>(out));
   }
   static const BatchImpl* get() {
-    static const BatchImpl impl = {iterate,     clear, init, quantity, blocks_per_sm, tile_kernel,
-                                   pairs ? M::PAIR_THREADS : 0, sizeof(R), M::Q, M::NG, M::NSET, M::NZS,
+    static const BatchImpl impl = {iterate,
+                                   tma_grid,
+                                   derive,
+                                   clear,
+                                   init,
+                                   quantity,
+                                   blocks_per_sm,
+                                   tile_kernel,
+                                   pairs ? M::PAIR_THREADS : 0,
+                                   M::has_bulk,
+                                   sizeof(R),
+                                   M::Q,
+                                   M::NG,
+                                   M::NSET,
+                                   M::NZS,
                                    M::ZONE_SHIFT};
     return &impl;
   }
@@ -166,9 +229,11 @@ size_t elem_size(int precision, int storage) {
 }
 
 struct CaseLayout {
-  size_t stride, buf, flags, zone, glob, total;
+  size_t stride, buf, flags, zone, glob, maps, total;
 };
 
+// One allocation per case: two snapshots, node types, zone table, Globals,
+// and for a case the tile-staged kernel can take, its tensor maps.
 CaseLayout case_layout(const BatchImpl* I, size_t elem, int nx, int ny, int nz) {
   CaseLayout L;
   const size_t N = (size_t)nx * ny * nz;
@@ -177,13 +242,16 @@ CaseLayout case_layout(const BatchImpl* I, size_t elem, int nx, int ny, int nz) 
   L.flags = align_up(N * sizeof(flag_t), 256);
   L.zone = align_up((size_t)(1 << (16 - I->zone_shift)) * I->NZS * I->real_size, 256);
   L.glob = align_up(I->NG * sizeof(double), 256);
-  L.total = 2 * L.buf + L.flags + L.zone + L.glob;
+  L.maps = tma_rows_for(elem, nx, ny) ? align_up(sizeof(BatchTmaMaps), 256) : 0;
+  L.total = 2 * L.buf + L.flags + L.zone + L.glob + L.maps;
   return L;
 }
 
-__global__ void k_batch_status(const BatchCase* cases, int n, int2* status) {
+// Per case (iterations done, left), then (error word of the staging waits, 0).
+__global__ void k_batch_status(const BatchCase* cases, int n, const int* err, int2* status) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < n) status[c] = make_int2(cases[c].counter, cases[c].remaining);
+  else if (c == n) status[n] = make_int2(*err, 0);
 }
 
 }  // namespace
@@ -198,23 +266,33 @@ struct tclb_batch {
   BatchCase* d_cases = nullptr;
   int2* d_status = nullptr;
   int2* h_status = nullptr;  // pinned
-  int* d_ntiles = nullptr;
+  int* d_ntiles = nullptr;   // [0] tiles of the cases not staged, [1] all tiles, [2] staged tiles
+  int* d_err = nullptr;      // staging wait ran out
   BatchTile* d_tiles = nullptr;
-  size_t tiles_cap = 0;
+  BatchTmaTile* d_ttiles = nullptr;
+  size_t tiles_cap = 0, ttiles_cap = 0;
   std::vector<BatchCase> cases;
   std::vector<size_t> bytes;
   std::vector<char> used_slot;
   bool tiles_dirty = true;
-  int ntiles = 0;
+  int ntiles = 0, nplain = 0, nttiles = 0;
   int bx = 128, by = 2, K = 16, grid_blocks = 0, user_grid = 0;
   int sms = 148;   // multiprocessors of the device
   int tile_h = 0;  // height of the tiles in the table
+  int tma_grid = -1;  // resident blocks of the tile-staged kernel (-1: not yet asked)
+  // Settings of the staged group: for models with the packed collision the
+  // tile-staged launch takes its settings as kernel parameters, so only the
+  // cases with these settings are staged (the others take the pair kernel).
+  // Chosen when the tile table is rebuilt: kept while a live case has them.
+  std::vector<double> group;
+  int status_n = -1;  // cases in the status read back by the last step (its error word follows)
   cudaGraphExec_t graph = nullptr;
-  cudaGraph_t graph_src = nullptr;            // kept: its nodes address the instantiated graph
-  std::vector<cudaGraphNode_t> iter_nodes;    // the K iteration launches (one block per tile)
-  int graph_grid = 0;                         // their grid size in the instantiated graph
-  int graph_key[6] = {-1, -1, -1, -1, -1, -1};
-  int paths = TCLB_LAUNCH_PAIRS | TCLB_BATCH_SHORT_TILES;  // tclb_batch_set_paths
+  cudaGraph_t graph_src = nullptr;          // kept: its nodes address the instantiated graph
+  std::vector<cudaGraphNode_t> plain_nodes;  // one-block-per-tile plain launches
+  std::vector<cudaGraphNode_t> glob_nodes;   // the Globals launch
+  int graph_grid[2] = {0, 0};                // their grids in the instantiated graph
+  int graph_key[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+  int paths = TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES;  // tclb_batch_set_paths
 };
 
 namespace {
@@ -232,6 +310,25 @@ bool pair_form(const tclb_batch* B) {
          B->bx / 2 <= B->I->pair_threads;
 }
 
+bool in_group(const tclb_batch* B, const BatchCase& C) {
+  if (!B->I->group_staging) return true;
+  if ((int)B->group.size() != B->I->NSET) return false;
+  for (int i = 0; i < B->I->NSET; i++)
+    if (C.s[i] != B->group[i]) return false;
+  return true;
+}
+
+// Plain launches of this case take the tile-staged kernel: staging enabled,
+// one block per tile, the case fits it (tensor maps were made) and belongs
+// to the staged group.
+bool staged(const tclb_batch* B, const BatchCase& C) {
+  return (B->paths & TCLB_LAUNCH_TMA) && B->user_grid == 0 && C.tma_rows > 0 && B->tma_grid > 0 && in_group(B, C);
+}
+
+bool live(const tclb_batch* B, size_t s) {
+  return B->used_slot[s] && B->cases[s].active && B->h_status[s].y > 0;  // finished cases get no tiles
+}
+
 // Tile height: the set by, halved (down to the block's thread rows) while
 // the live cases would give fewer tiles than two waves of resident blocks --
 // a few small cases alone run as many short tiles, not a few long ones.
@@ -246,8 +343,7 @@ int tile_height(const tclb_batch* B) {
     size_t n = 0;
     for (size_t s = 0; s < B->cases.size(); s++) {
       const BatchCase& C = B->cases[s];
-      if (!B->used_slot[s] || !C.active || B->h_status[s].y <= 0) continue;
-      n += (size_t)C.nz * ((C.ny + h - 1) / h) * ((C.nx + B->bx - 1) / B->bx);
+      if (live(B, s) && !staged(B, C)) n += (size_t)C.nz * ((C.ny + h - 1) / h) * ((C.nx + B->bx - 1) / B->bx);
     }
     return n;
   };
@@ -256,51 +352,101 @@ int tile_height(const tclb_batch* B) {
   return h;
 }
 
-int rebuild_tiles(tclb_batch* B) {
-  std::vector<BatchTile> t;
-  const int h = tile_height(B);
+// Grow a device table (pool memory) to hold n entries; a move forces a recapture.
+template <class E>
+int reserve(tclb_batch* B, E*& d, size_t& cap, size_t n) {
+  if (n <= cap) return TCLB_OK;
+  if (d) BCK(cudaFreeAsync(d, B->stream));
+  cap = std::max(n, cap * 2);
+  BCK(cudaMallocFromPoolAsync((void**)&d, cap * sizeof(E), B->pool, B->stream));
+  B->graph_key[0] = -1;
+  return TCLB_OK;
+}
+
+// The tile tables: bx x h tiles of the cases not staged, then those of the
+// staged cases (the Globals launch covers both), and the staged cases'
+// R-row tiles.
+// The staged group: kept while a live case that fits the tile-staged kernel
+// has its settings, else the settings of the first such case.
+void choose_group(tclb_batch* B) {
+  if (!B->I->group_staging) return;
+  const BatchCase* first = nullptr;
   for (size_t s = 0; s < B->cases.size(); s++) {
     const BatchCase& C = B->cases[s];
-    if (!B->used_slot[s] || !C.active || B->h_status[s].y <= 0) continue;  // finished cases get no tiles
-    for (int z = 0; z < C.nz; z++)
-      for (int y = 0; y < C.ny; y += h)
-        for (int x = 0; x < C.nx; x += B->bx) t.push_back({(int)s, x, y, z, h});
+    if (!live(B, s) || C.tma_rows == 0) continue;
+    if (in_group(B, C)) return;
+    if (!first) first = &C;
+  }
+  if (first) {
+    B->group.assign(first->s, first->s + B->I->NSET);
+    B->tiles_dirty = true;
+  }
+}
+
+int rebuild_tiles(tclb_batch* B) {
+  if (B->tma_grid < 0) B->tma_grid = B->I->tma_grid(B->sms);
+  choose_group(B);
+  std::vector<BatchTile> t;
+  std::vector<BatchTmaTile> tt;
+  const int h = tile_height(B);
+  for (int pass = 0; pass < 2; pass++) {  // the cases not staged, then the staged ones
+    for (size_t s = 0; s < B->cases.size(); s++) {
+      const BatchCase& C = B->cases[s];
+      if (!live(B, s) || staged(B, C) != (pass == 1)) continue;
+      for (int z = 0; z < C.nz; z++)
+        for (int y = 0; y < C.ny; y += h)
+          for (int x = 0; x < C.nx; x += B->bx) t.push_back({(int)s, x, y, z, h});
+      if (pass == 1)
+        for (int z = 0; z < C.nz; z++)
+          for (int y = 0; y < C.ny; y += C.tma_rows) tt.push_back({(int)s, z, y});
+    }
+    if (pass == 0) B->nplain = (int)t.size();
   }
   B->tile_h = h;
-  if (t.size() > B->tiles_cap) {
-    if (B->d_tiles) BCK(cudaFreeAsync(B->d_tiles, B->stream));
-    B->tiles_cap = std::max(t.size(), B->tiles_cap * 2);
-    BCK(cudaMallocFromPoolAsync((void**)&B->d_tiles, B->tiles_cap * sizeof(BatchTile), B->pool, B->stream));
-    B->graph_key[0] = -1;  // tile table moved: recapture
-  }
+  int rc;
+  if ((rc = reserve(B, B->d_tiles, B->tiles_cap, t.size())) || (rc = reserve(B, B->d_ttiles, B->ttiles_cap, tt.size())))
+    return rc;
   B->ntiles = (int)t.size();
+  B->nttiles = (int)tt.size();
   if (!t.empty())
     BCK(cudaMemcpyAsync(B->d_tiles, t.data(), t.size() * sizeof(BatchTile), cudaMemcpyHostToDevice, B->stream));
-  BCK(cudaMemcpyAsync(B->d_ntiles, &B->ntiles, sizeof(int), cudaMemcpyHostToDevice, B->stream));
-  BCK(cudaStreamSynchronize(B->stream));  // host vector t dies here
+  if (!tt.empty())
+    BCK(cudaMemcpyAsync(B->d_ttiles, tt.data(), tt.size() * sizeof(BatchTmaTile), cudaMemcpyHostToDevice,
+                        B->stream));
+  const int n[3] = {B->nplain, B->ntiles, B->nttiles};
+  BCK(cudaMemcpyAsync(B->d_ntiles, n, sizeof(n), cudaMemcpyHostToDevice, B->stream));
+  BCK(cudaStreamSynchronize(B->stream));  // the host vectors die here
   B->tiles_dirty = false;
   return TCLB_OK;
 }
 
-// One block per tile: the iteration launches' grid is the live tile count.
-// When only that changes, the K kernel nodes of the instantiated graph get
-// the new grid in place (no recapture).
+// One block per tile: the grid of the plain launches is the count of tiles
+// of the cases not staged, that of the Globals launch the count of all tiles.
+// When only those change, the kernel nodes of the instantiated graph get the
+// new grids in place (no recapture).
 int update_graph_grid(tclb_batch* B) {
-  const int grid = std::max(1, B->ntiles);
-  if (B->user_grid != 0 || grid == B->graph_grid) return TCLB_OK;
-  for (cudaGraphNode_t node : B->iter_nodes) {
-    cudaKernelNodeParams p;
-    BCK(cudaGraphKernelNodeGetParams(node, &p));
-    p.gridDim = dim3(grid);
-    BCK(cudaGraphExecKernelNodeSetParams(B->graph, node, &p));
+  if (B->user_grid != 0) return TCLB_OK;
+  const int grid[2] = {std::max(1, B->nplain), std::max(1, B->ntiles)};
+  for (int w = 0; w < 2; w++) {
+    if (grid[w] == B->graph_grid[w]) continue;
+    for (cudaGraphNode_t node : (w ? B->glob_nodes : B->plain_nodes)) {
+      cudaKernelNodeParams p;
+      BCK(cudaGraphKernelNodeGetParams(node, &p));
+      p.gridDim = dim3(grid[w]);
+      BCK(cudaGraphExecKernelNodeSetParams(B->graph, node, &p));
+    }
+    B->graph_grid[w] = grid[w];
   }
-  B->graph_grid = grid;
   return TCLB_OK;
 }
 
 int ensure_graph(tclb_batch* B) {
-  const int key[6] = {B->bx, B->by, B->K, (int)B->cases.size(), B->user_grid, B->paths};
-  if (B->graph && std::equal(key, key + 6, B->graph_key)) return update_graph_grid(B);
+  const int has_tma = B->nttiles > 0;
+  // the staged group's settings are captured as kernel parameters
+  const int group_hash = (int)std::hash<std::string>()(
+      std::string(reinterpret_cast<const char*>(B->group.data()), B->group.size() * sizeof(double)));
+  const int key[8] = {B->bx, B->by, B->K, (int)B->cases.size(), B->user_grid, B->paths, has_tma, group_hash};
+  if (B->graph && std::equal(key, key + 8, B->graph_key)) return update_graph_grid(B);
   if (B->graph) {
     cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
@@ -309,27 +455,28 @@ int ensure_graph(tclb_batch* B) {
     cudaGraphDestroy(B->graph_src);
     B->graph_src = nullptr;
   }
-  B->iter_nodes.clear();
-  int dev = B->device, sms = 148, per_sm = 4;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  B->plain_nodes.clear();
+  B->glob_nodes.clear();
   const int threads = B->bx * block_rows(B->bx, B->by, 256);
-  per_sm = B->I->blocks_per_sm(threads);
+  int per_sm = B->I->blocks_per_sm(threads);
   if (per_sm < 1) per_sm = std::max(1, 2048 / threads);
   // grid_blocks 0 (default): one block per live tile; > 0: a persistent grid
   // of that size walking the tiles; < 0: persistent, SMs x resident blocks.
   const bool per_tile = B->user_grid == 0;
-  B->grid_blocks = per_tile ? std::max(1, B->ntiles) : (B->user_grid > 0 ? B->user_grid : sms * per_sm);
+  B->grid_blocks = per_tile ? std::max(1, B->nplain) : (B->user_grid > 0 ? B->user_grid : B->sms * per_sm);
+  const int grid_all = per_tile ? std::max(1, B->ntiles) : B->grid_blocks;
   const int form = !per_tile ? FORM_PERSISTENT : (pair_form(B) ? FORM_PAIR : FORM_TILE);
+  const LaunchTables L = {B->d_cases, B->d_tiles, B->d_ntiles, B->d_ttiles, B->d_ntiles + 2, B->d_err};
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   const int n = (int)B->cases.size();
   B->I->clear(B->d_cases, n, B->stream);
   for (int k = 0; k < B->K; k++)
-    B->I->iterate(B->d_cases, B->d_tiles, B->d_ntiles, k, B->K, dim3(B->grid_blocks), B->bx, B->by, form,
-                  B->stream);
+    B->I->iterate(L, k, B->K, dim3(B->grid_blocks), dim3(grid_all), has_tma ? B->tma_grid : 0,
+                  B->group.empty() ? nullptr : B->group.data(), B->bx, B->by, form, B->stream);
   if (n > 0) {
     k_batch_advance<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->K);
-    k_batch_status<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->d_status);
+    k_batch_status<<<(n + 128) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->d_err, B->d_status);
   }
   cudaError_t e = cudaStreamEndCapture(B->stream, &g);
   if (e != cudaSuccess) return bfail(TCLB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -339,7 +486,7 @@ int ensure_graph(tclb_batch* B) {
     return bfail(TCLB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   B->graph_src = g;
-  if (per_tile) {  // remember the iteration launches, to resize their grid later
+  if (per_tile) {  // remember the one-block-per-tile launches, to resize their grids later
     size_t count = 0;
     BCK(cudaGraphGetNodes(g, nullptr, &count));
     std::vector<cudaGraphNode_t> nodes(count);
@@ -353,11 +500,13 @@ int ensure_graph(tclb_batch* B) {
       if (type != cudaGraphNodeTypeKernel) continue;
       cudaKernelNodeParams p;
       BCK(cudaGraphKernelNodeGetParams(node, &p));
-      if (p.func == f0 || p.func == f1 || (f2 && p.func == f2)) B->iter_nodes.push_back(node);
+      if (p.func == f0 || (f2 && p.func == f2)) B->plain_nodes.push_back(node);
+      else if (p.func == f1) B->glob_nodes.push_back(node);
     }
   }
-  B->graph_grid = B->grid_blocks;
-  std::copy(key, key + 6, B->graph_key);
+  B->graph_grid[0] = B->grid_blocks;
+  B->graph_grid[1] = grid_all;
+  std::copy(key, key + 8, B->graph_key);
   return TCLB_OK;
 }
 
@@ -403,11 +552,14 @@ int tclb_batch_create(tclb_batch_h* out, int model, int precision, int storage, 
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_cases, sizeof(BatchCase) * max_cases);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_status, sizeof(int2) * max_cases);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_ntiles, sizeof(int));
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&B->h_status, sizeof(int2) * max_cases);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_status, sizeof(int2) * (max_cases + 1));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_ntiles, 3 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&B->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(B->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&B->h_status, sizeof(int2) * (max_cases + 1));
+  if (e == cudaSuccess) std::memset(B->h_status, 0, sizeof(int2) * (max_cases + 1));
   if (e == cudaSuccess) e = cudaMemset(B->d_cases, 0, sizeof(BatchCase) * max_cases);
-  if (e == cudaSuccess) e = cudaMemset(B->d_ntiles, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(B->d_ntiles, 0, 3 * sizeof(int));
   if (e != cudaSuccess) {
     tclb_batch_destroy(B);
     return bfail(TCLB_ERR_CUDA, std::string("batch create: ") + cudaGetErrorString(e));
@@ -424,10 +576,12 @@ int tclb_batch_destroy(tclb_batch_h B) {
   for (size_t s = 0; s < B->cases.size(); s++)
     if (B->used_slot[s]) cudaFreeAsync(B->cases[s].buf[0], B->stream);
   if (B->d_tiles) cudaFreeAsync(B->d_tiles, B->stream);
+  if (B->d_ttiles) cudaFreeAsync(B->d_ttiles, B->stream);
   if (B->stream) cudaStreamSynchronize(B->stream);
   if (B->d_cases) cudaFree(B->d_cases);
   if (B->d_status) cudaFree(B->d_status);
   if (B->d_ntiles) cudaFree(B->d_ntiles);
+  if (B->d_err) cudaFree(B->d_err);
   if (B->h_status) cudaFreeHost(B->h_status);
   if (B->pool) cudaMemPoolDestroy(B->pool);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -474,7 +628,22 @@ int tclb_batch_add_case(tclb_batch_h B, int nx, int ny, int nz, const uint16_t* 
   C.counter = 0;
   C.remaining = niter;
   C.active = 1;
+  BatchTmaMaps maps;  // host copy of the tensor maps, uploaded below
+  if (L.maps) {
+    const int R = tma_rows_for(B->elem, nx, ny);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; b++)
+      ok = encode_tile_maps(C.buf[b], C.flags, nx, ny, nz, B->I->Q, L.stride, R, &maps.rows[b], &maps.row1[b],
+                            &maps.flags);
+    if (ok) {  // otherwise the case runs the register kernels
+      C.tma_rows = R;
+      C.maps = reinterpret_cast<const BatchTmaMaps*>(p + 2 * L.buf + L.flags + L.zone + L.glob);
+      BCK(cudaMemcpyAsync(const_cast<BatchTmaMaps*>(C.maps), &maps, sizeof(maps), cudaMemcpyHostToDevice,
+                          B->stream));
+    }
+  }
   for (int i = 0; i < T->nsettings && i < BATCH_MAX_SET; i++) C.s[i] = settings[i];
+  B->I->derive(C);
   // zonal table: default values, then the caller's rows (zone 0.. zone_rows-1)
   const int nzs = T->nzonesettings;
   std::vector<double> zt((size_t)nzones * nzs);
@@ -537,7 +706,7 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
   CHECK_B(B);
   if (bx < 32 || bx % 32 || bx > 256 || by < 1 || by > 256 || iters_per_launch < 1 || iters_per_launch > 4096)
     return bfail(TCLB_ERR_ARG, "bad launch shape");
-  if (bx != B->bx || by != B->by) B->tiles_dirty = true;
+  B->tiles_dirty = true;  // the shape and the grid form decide the tables
   B->bx = bx;
   B->by = by;
   B->K = iters_per_launch;
@@ -548,8 +717,9 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
 
 int tclb_batch_set_paths(tclb_batch_h B, int flags) {
   CHECK_B(B);
-  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_BATCH_SHORT_TILES)) return bfail(TCLB_ERR_ARG, "unknown path flags");
-  if ((flags ^ B->paths) & TCLB_BATCH_SHORT_TILES) B->tiles_dirty = true;
+  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES))
+    return bfail(TCLB_ERR_ARG, "unknown path flags");
+  if (flags != B->paths) B->tiles_dirty = true;
   B->paths = flags;
   B->graph_key[0] = -1;
   return TCLB_OK;
@@ -557,7 +727,13 @@ int tclb_batch_set_paths(tclb_batch_h B, int flags) {
 
 int tclb_batch_get_paths(tclb_batch_h B, int* flags) {
   CHECK_B(B);
-  if (flags) *flags = (pair_form(B) ? TCLB_LAUNCH_PAIRS : 0) | (B->paths & TCLB_BATCH_SHORT_TILES);
+  if (B->tma_grid < 0) B->tma_grid = B->I->tma_grid(B->sms);
+  choose_group(B);
+  bool any_staged = false;
+  for (size_t s = 0; s < B->cases.size(); s++) any_staged |= live(B, s) && staged(B, B->cases[s]);
+  if (flags)
+    *flags = (pair_form(B) ? TCLB_LAUNCH_PAIRS : 0) | (any_staged ? TCLB_LAUNCH_TMA : 0) |
+             (B->paths & TCLB_BATCH_SHORT_TILES);
   return TCLB_OK;
 }
 
@@ -578,7 +754,8 @@ int tclb_batch_step(tclb_batch_h B) {
   if (B->cases.empty() || B->ntiles == 0) return TCLB_OK;
   if ((rc = ensure_graph(B))) return rc;
   BCK(cudaGraphLaunch(B->graph, B->stream));
-  BCK(cudaMemcpyAsync(B->h_status, B->d_status, sizeof(int2) * B->cases.size(), cudaMemcpyDeviceToHost,
+  B->status_n = (int)B->cases.size();
+  BCK(cudaMemcpyAsync(B->h_status, B->d_status, sizeof(int2) * (B->status_n + 1), cudaMemcpyDeviceToHost,
                       B->stream));
   return TCLB_OK;
 }
@@ -594,6 +771,12 @@ int tclb_batch_done(tclb_batch_h B) {
 int tclb_batch_sync(tclb_batch_h B) {
   CHECK_B(B);
   BCK(cudaStreamSynchronize(B->stream));
+  if (B->status_n >= 0 && B->h_status[B->status_n].x != 0) {  // a staging wait ran out
+    B->h_status[B->status_n].x = 0;
+    BCK(cudaMemsetAsync(B->d_err, 0, sizeof(int), B->stream));
+    BCK(cudaStreamSynchronize(B->stream));
+    return bfail(TCLB_ERR_CUDA, "tile pipeline: a wait for staged tiles ran out; the batch state is not valid");
+  }
   // cases that finished in the last step leave the tile table
   for (size_t s = 0; s < B->cases.size(); s++)
     if (B->used_slot[s] && B->cases[s].active && B->h_status[s].y <= 0 && B->cases[s].remaining > 0) {

@@ -84,6 +84,7 @@ struct StoreBF16 {
 // ---------------------------------------------------------------------------
 template <class R, int NSET>
 struct Args {
+  typedef R real;
   const void* src;
   void* dst;
   size_t stride;  // elements between population planes
@@ -115,10 +116,10 @@ struct D2Q9 {
   static constexpr int BATCH_MIN_BLOCKS = 6;  // one-tile batch kernel: <= 40 registers
   __device__ __forceinline__ static bool collides(flag_t) { return false; }
   __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
-  template <class R>
-  __device__ __forceinline__ static void pre_collision(R (&)[Q], flag_t, const Args<R, NSET>&) {}
-  template <bool DEV, class R>
-  __device__ __forceinline__ static void collide_pair(F2 (&)[Q], flag_t, flag_t, const Args<R, NSET>&) {}
+  template <class R, class AR>
+  __device__ __forceinline__ static void pre_collision(R (&)[Q], flag_t, const AR&) {}
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair(F2 (&)[Q], flag_t, flag_t, const AR&) {}
   template <class R>
   __host__ __device__ static void derived(const R*, R* k) { k[0] = k[1] = k[2] = k[3] = R(0); }
   __host__ __device__ static constexpr int ex(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0); }
@@ -415,8 +416,8 @@ struct D3Q19 {
   // deviations g = f - w: the sum of g is rho - 1, which enters the
   // equilibrium's terms linear in rho (giving feq - w), while the quadratic
   // terms and the force use the true density.
-  template <bool DEV = false, class V, class R>
-  __device__ __forceinline__ static void trt(V (&f)[Q], const Args<R, NSET>& a, V& rho, V& jx, V& jy, V& jz) {
+  template <bool DEV = false, class V, class AR>
+  __device__ __forceinline__ static void trt(V (&f)[Q], const AR& a, V& rho, V& jx, V& jy, V& jz) {
     V s[9], d[9];
 #pragma unroll
     for (int p = 0; p < 9; p++) {
@@ -481,8 +482,8 @@ struct D3Q19 {
   }
 
   // BOUNDARY group of Run (:181-204)
-  template <class R>
-  __device__ __forceinline__ static void boundaries(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
+  template <class R, class AR>
+  __device__ __forceinline__ static void boundaries(R (&f)[Q], flag_t fl, const AR& a) {
     const unsigned b = fl & d3q19::BOUNDARY;
     if (b) {
       switch (b) {  // :181-204
@@ -537,12 +538,12 @@ struct D3Q19 {
   // its values; the rates are the same for every node).
   __device__ __forceinline__ static bool collides(flag_t fl) { return (fl & d3q19::COLLISION) == d3q19::MRT; }
   __device__ __forceinline__ static bool has_boundary(flag_t fl) { return (fl & d3q19::BOUNDARY) != 0; }
-  template <class R>
-  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
+  template <class R, class AR>
+  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const AR& a) {
     boundaries(f, fl, a);
   }
-  template <bool DEV, class R>
-  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const Args<R, NSET>& a) {
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const AR& a) {
     F2 rho, jx, jy, jz;
     trt<DEV>(f, a, rho, jx, jy, jz);
   }
@@ -730,8 +731,8 @@ struct D3Q27C {
     // Cumulants of order >= 4 are set to zero by the collision and those of
     // order 3 are scaled by (1 - Omega): with the default Omega = 1 they vanish
     // too, so only orders <= 2 are converted (a branch uniform over the launch).
-    if (a.s[d3q27c::S_Omega] == R(1)) relax<R, R, false>(f, a, w0);
-    else relax<R, R, true>(f, a, w0);
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<R, Args<R, NSET>, false>(f, a, w0);
+    else relax<R, Args<R, NSET>, true>(f, a, w0);
     from_raw(f);
   }
 
@@ -766,8 +767,8 @@ struct D3Q27C {
   __device__ __forceinline__ static bool has_boundary(flag_t fl) {
     return (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) != 0;
   }
-  template <class R>
-  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const Args<R, NSET>& a) {
+  template <class R, class AR>
+  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const AR& a) {
     if (fl & (d3q27c::ADDITIONALS | d3q27c::BOUNDARY)) {
       R g[1];
       boundaries<R, false>(f, fl, g, a.zone + (fl >> ZONE_SHIFT) * NZS);
@@ -789,20 +790,22 @@ struct D3Q27C {
     m[24] += V(sign * (1.0f / 9.0f));
     m[26] += V(sign * (1.0f / 27.0f));
   }
-  template <bool DEV, class R>
-  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t fla, flag_t flb, const Args<R, NSET>& a) {
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t fla, flag_t flb, const AR& a) {
+    typedef typename AR::real R;
     const F2 w0((float)((fla & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]), (float)((flb & d3q27c::BOUNDARY) ? a.k[1] : a.k[0]));
     to_raw(f);
     if (DEV) weight_moments(f, 1.0f);
-    if (a.s[d3q27c::S_Omega] == R(1)) relax<F2, R, false>(f, a, w0);
-    else relax<F2, R, true>(f, a, w0);
+    if (a.s[d3q27c::S_Omega] == R(1)) relax<F2, AR, false>(f, a, w0);
+    else relax<F2, AR, true>(f, a, w0);
     if (DEV) weight_moments(f, -1.0f);
     from_raw(f);
   }
 
   // Raw moments f -> cumulants -> relaxed cumulants -> raw moments (:359-477).
-  template <class V, class R, bool THIRD>
-  __device__ __forceinline__ static void relax(V (&f)[Q], const Args<R, NSET>& a, V w0) {
+  template <class V, class AR, bool THIRD>
+  __device__ __forceinline__ static void relax(V (&f)[Q], const AR& a, V w0) {
+    typedef typename AR::real R;
     const V Fx = V(a.s[d3q27c::S_ForceX]), Fy = V(a.s[d3q27c::S_ForceY]), Fz = V(a.s[d3q27c::S_ForceZ]);
     const V w1 = V(1);
     V c[Q];
@@ -1032,9 +1035,11 @@ struct Pack16<StoreBF16<SH>> {
 // Models with a packed collision: boundary conditions per node, then one
 // FP32x2 collision for both; others: the scalar node update twice. Plain
 // iterations (no Globals).
-template <class M, class R, class St, class A>
-__device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb,
-                                                  const Args<R, M::NSET>& a, const A& P, unsigned node) {
+// AR: Args<R, M::NSET>, or for the packed models a view with the same
+// members s[], k[], zone (SharedArgsView).
+template <class M, class R, class St, class A, class AR>
+__device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb, const AR& a, const A& P,
+                                                  unsigned node) {
   using P16 = Pack16<St>;
   if constexpr (M::has_bulk && sizeof(R) == 4) {
     // Values stay packed (node x, node x+1). A node with a boundary type has

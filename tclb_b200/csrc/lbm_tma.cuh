@@ -26,6 +26,7 @@
 // the other warps' waits then run out in turn, so the kernel always ends.
 #pragma once
 #include <cuda.h>
+#include <cuda_runtime.h>
 
 #include "lbm_kernels.cuh"
 
@@ -36,6 +37,65 @@ struct TmaMaps {
   CUtensorMap row1;  // same tensor, box (nx, 1, 1, 1)
   CUtensorMap flags;  // node types: dims (nx, ny, nz), box (nx, R, 1)
 };
+
+// Rows per tile of a lattice for the tile-staged kernels: 16-bit storage, nx
+// a multiple of 64 up to 256 (a row is one TMA box), R = 512 / nx dividing
+// ny; 0 where they do not apply.
+inline int tma_rows_for(size_t elem, int nx, int ny) {
+  if (elem != 2 || nx % 64 || nx > 256) return 0;
+  const int R = 512 / nx;
+  return ny % R ? 0 : R;
+}
+
+// The driver's cuTensorMapEncodeTiled, reached through the runtime's
+// entry-point query so the library links only the runtime; null if absent.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+inline EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    EncodeTiledFn f = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      f = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+    return f;
+  }();
+  return fn;
+}
+
+// The three maps of one snapshot (16-bit values, planes `stride` apart) and
+// its node types: rows (nx, ny, nz, Q) with an (nx, R, 1, 1) box, the same
+// tensor with a one-row box, and the node types (nx, ny, nz) with an
+// (nx, R, 1) box. False if the encoder is missing or refuses.
+inline bool encode_tile_maps(void* buf, const void* flags, int nx, int ny, int nz, int Q, size_t stride, int R,
+                             CUtensorMap* rows, CUtensorMap* row1, CUtensorMap* fmap) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t e = 2;
+  const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
+  const cuuint64_t strides[3] = {nx * e, (cuuint64_t)nx * ny * e, stride * e};
+  const cuuint32_t box_rows[4] = {(cuuint32_t)nx, (cuuint32_t)R, 1, 1};
+  const cuuint32_t box_row1[4] = {(cuuint32_t)nx, 1, 1, 1};
+  const cuuint32_t ones[4] = {1, 1, 1, 1};
+  if (enc(rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, buf, dims, strides, box_rows, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if (enc(row1, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, buf, dims, strides, box_row1, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint64_t fdims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t fstrides[2] = {nx * e, (cuuint64_t)nx * ny * e};
+  const cuuint32_t fbox[3] = {(cuuint32_t)nx, (cuuint32_t)R, 1};
+  return enc(fmap, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(flags), fdims, fstrides, fbox, ones,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // Stages (shared memory per block: 128 + 3 * (Q+1) * 1 KB), two blocks per
 // SM. Three suffice: for d3q19, whose tiles compute fastest, 4 and 5 stages
@@ -100,16 +160,15 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Issue the copies of tile t into one stage; called by the whole producer
-// warp after lane 0 has armed the stage's full barrier. Lane i < Q copies
-// population i (one R-row box, or R one-row boxes where the rows wrap at a
-// y face), lane Q the node types.
+// Issue the copies of the tile of rows y0 .. y0+R-1 of plane z into one
+// stage; called by the whole producer warp after lane 0 has armed the stage's
+// full barrier. Lane i < Q copies population i (one R-row box, or R one-row
+// boxes where the rows wrap at a y face), lane Q the node types.
 template <class M>
-__device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage, unsigned bar, int t, int nx,
-                                         int ny, int nz, int R, int lane) {
-  const int rows_per_plane = ny / R;
-  const int z = t / rows_per_plane, y0 = (t % rows_per_plane) * R;
-  constexpr unsigned block = TMA_TILE;  // values per population block (R * nx)
+__device__ __forceinline__ void tma_fill_at(const CUtensorMap* rows, const CUtensorMap* row1,
+                                            const CUtensorMap* flags, unsigned short* stage, unsigned bar, int z,
+                                            int y0, int nx, int ny, int nz, int R, int lane) {
+  constexpr unsigned block = TMA_TILE;  // values per population block (R * nx at most)
   if (lane < M::Q) {
     const int i = lane;
     const int ey = M::ey(i), ez = M::DIM == 2 ? 0 : M::ez(i);
@@ -118,17 +177,26 @@ __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage
     const unsigned dst = smem_u32(stage + (size_t)i * block);
     const int ys = y0 - ey;
     if (ys >= 0 && ys + R <= ny) {
-      tma_load_4d(dst, &T.rows, 0, ys, zs, i, bar);
+      tma_load_4d(dst, rows, 0, ys, zs, i, bar);
     } else {  // rows wrap at a y face: one row at a time
       for (int r = 0; r < R; r++) {
         int y = ys + r;
         y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-        tma_load_4d(dst + (unsigned)(r * nx * 2), &T.row1, 0, y, zs, i, bar);
+        tma_load_4d(dst + (unsigned)(r * nx * 2), row1, 0, y, zs, i, bar);
       }
     }
   } else if (lane == M::Q) {
-    tma_load_3d(smem_u32(stage + (size_t)M::Q * block), &T.flags, 0, y0, z, bar);
+    tma_load_3d(smem_u32(stage + (size_t)M::Q * block), flags, 0, y0, z, bar);
   }
+}
+
+// Tile t of a lattice (tiles of R rows, z-major).
+template <class M>
+__device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage, unsigned bar, int t, int nx,
+                                         int ny, int nz, int R, int lane) {
+  const int rows_per_plane = ny / R;
+  const int z = t / rows_per_plane, y0 = (t % rows_per_plane) * R;
+  tma_fill_at<M>(&T.rows, &T.row1, &T.flags, stage, bar, z, y0, nx, ny, nz, R, lane);
 }
 
 // The kernel: ncons = R*nx/64 = TMA_CONSUMERS warps update node pairs, one

@@ -322,60 +322,18 @@ const Impl* impl_for(int model, int precision, int storage) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Tensor maps of the tile-staged kernel (16-bit storage, nx a multiple of 64
-// and at most 256, R = 512 / nx rows per tile dividing ny). The encoder is the
-// driver's cuTensorMapEncodeTiled, reached through the runtime's entry-point
-// query so the library links only the runtime. When anything does not fit,
-// tma_ok stays 0 and the register kernels run.
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-    cudaGetLastError();
-  });
-  return fn;
-}
-
+// and at most 256, R = 512 / nx rows per tile dividing ny). When anything
+// does not fit, tma_ok stays 0 and the register kernels run.
 void setup_tma(tclb_lattice* L) {
   L->tma_ok = 0;
   // Tiles of 512 nodes (R whole rows). Longer rows take the register pair
   // kernel: one-row tiles copied in two boxes measured slower than it.
-  if (L->elem != 2 || L->nx % 64 || L->nx > 256) return;
-  const int R = (int)TMA_TILE / L->nx;
-  if (L->ny % R) return;
-  EncodeTiledFn enc = encode_tiled();
-  if (!enc) return;
-  const cuuint64_t e = 2;
-  const cuuint64_t dims[4] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz, (cuuint64_t)L->T->Q};
-  const cuuint64_t strides[3] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e, L->stride * e};
-  const cuuint32_t box_rows[4] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1, 1};
-  const cuuint32_t box_row1[4] = {(cuuint32_t)L->nx, 1, 1, 1};
-  const cuuint32_t ones[4] = {1, 1, 1, 1};
-  for (int b = 0; b < 2; b++) {
-    if (enc(&L->tma[b].rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, L->buf[b], dims, strides, box_rows, ones,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+  const int R = tma_rows_for(L->elem, L->nx, L->ny);
+  if (!R) return;
+  for (int b = 0; b < 2; b++)
+    if (!encode_tile_maps(L->buf[b], L->flags, L->nx, L->ny, L->nz, L->T->Q, L->stride, R, &L->tma[b].rows,
+                          &L->tma[b].row1, &L->tma[b].flags))
       return;
-    if (enc(&L->tma[b].row1, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, L->buf[b], dims, strides, box_row1, ones,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return;
-    const cuuint64_t fdims[3] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz};
-    const cuuint64_t fstrides[2] = {L->nx * e, (cuuint64_t)L->nx * L->ny * e};
-    const cuuint32_t fbox[3] = {(cuuint32_t)L->nx, (cuuint32_t)R, 1};
-    if (enc(&L->tma[b].flags, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, L->flags, fdims, fstrides, fbox, ones,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return;
-  }
   L->tma_rows = R;
   L->tma_ok = 1;
 }

@@ -262,3 +262,65 @@ def test_short_tiles_when_few():
         b.close()
     assert res[1][0] == 2 and res[0][0] == 2 * 64 // 4  # short: 4-row tiles (the block's thread rows)
     assert np.array_equal(res[0][1], res[1][1])
+
+
+TMA_SHAPES = {
+    "d2q9": [(1, 16, 64), (1, 8, 128), (1, 6, 192), (1, 10, 96)],
+    "d3q19": [(4, 16, 64), (3, 12, 128), (2, 10, 192), (2, 6, 256), (3, 8, 96)],
+    "d3q27_cumulant": [(3, 16, 64), (2, 8, 128), (2, 4, 192), (3, 8, 96)],
+}
+
+
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+@pytest.mark.parametrize("storage", ["fp16s", "bf16"])
+def test_batch_tile_staged_matches_pairs_bit_for_bit(model, storage):
+    """Cases whose rows fit one TMA box (nx 64, 128, 192, 256) take the
+    tile-staged batch kernel, the others (nx = 96) the pair kernel, in one
+    batch; every field and Globals vector must equal that of the same batch
+    with staging off (the same pair update on the same values)."""
+    specs = [_random_case(model, sh, seed=41 + i, niter=9) for i, sh in enumerate(TMA_SHAPES[model])]
+    # a case that fits the staged kernel but has other settings: for the
+    # packed-collision models it leaves the staged group and takes the pairs
+    odd = _random_case(model, TMA_SHAPES[model][0], seed=49, niter=9)
+    odd.settings[next(iter(odd.settings))] *= 1.25
+    specs.append(odd)
+    out = []
+    for tma in (True, False):
+        b = Batch(model, "fp32", storage=storage, budget_bytes=1 << 30)
+        b.set_launch(64, 4, 4)  # K does not divide the iteration count
+        b.set_paths(use_tma=tma)
+        ids = [b.add_case(s) for s in specs]
+        assert b.uses_tma() == tma and b.uses_pairs()
+        b.run_to_completion()
+        out.append([(b.quantity(c, "U"), b.quantity(c, M.get(model).quantities[0][0]), b.globals(c)) for c in ids])
+        b.close()
+    for (u0, p0, g0), (u1, p1, g1) in zip(*out):
+        assert np.isfinite(u0).all()
+        assert np.array_equal(u0, u1) and np.array_equal(p0, p1)
+        assert np.array_equal(g0, g1)
+
+
+def test_batch_tile_staged_late_admission_and_retire():
+    """Staged and unstaged d3q19 cases joining and leaving between replays
+    (the staged tile table is rebuilt, the graph's grids resized): each result
+    equals that of the case alone in a batch with staging off."""
+    specs = [_random_case("d3q19", sh, seed=51 + i, niter=n)
+             for i, (sh, n) in enumerate([((4, 16, 64), 13), ((3, 8, 96), 6), ((2, 12, 128), 20)])]
+    b = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=1 << 30)
+    b.set_launch(64, 8, 5)
+    c0 = b.add_case(specs[0])
+    c1 = b.add_case(specs[1])
+    b.step()
+    b.sync()
+    c2 = b.add_case(specs[2])
+    b.run_to_completion()
+    got = [b.quantity(c, "U") for c in (c0, c1, c2)]
+    b.close()
+    for s, u in zip(specs, got):
+        a = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=1 << 30)
+        a.set_launch(64, 8, 5)
+        a.set_paths(use_tma=False)
+        c = a.add_case(s)
+        a.run_to_completion()
+        assert np.array_equal(a.quantity(c, "U"), u)
+        a.close()
