@@ -248,3 +248,61 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150)
         rep["fraction_of_single"] = t_ideal / rep["busy_s"] if rep["busy_s"] else 0.0
         out["runs"][st] = rep
     return out
+
+
+# ---------------------------------------------------------------------------
+# Profiling workloads: one porous d3q19 box (p = 0.08, 2-node wall band, seed
+# 1), n^3 nodes, advanced through a batch (its kernel path chosen by the
+# batch's paths) or through a single lattice. Small enough for an ncu capture.
+# ---------------------------------------------------------------------------
+def porous_box_batch(n=128, storage="fp16s", replays=3, K=8, bx=64, by=64, use_tma=True) -> dict:
+    import torch
+
+    b = Batch("d3q19", "fp32", storage=storage, budget_bytes=8 << 30, max_cases=2)
+    b.set_launch(bx, by, K)
+    b.set_paths(use_tma=use_tma)
+    fl = cases.porous_channel_d3q19(n, n, n, p=0.08, band=2, seed=1)
+    b.add_case(CaseSpec(fl, {"nu": 0.02, "ForceX": 1e-5}, {}, 1 << 20))
+    staged, pairs = b.uses_tma(), b.uses_pairs()
+    for _ in range(replays):
+        b.step()
+    b.sync()
+    torch.cuda.synchronize()
+    b.close()
+    return {"workload": f"batch, one d3q19 porous box {n}^3, {storage}", "replays": replays, "K": K,
+            "tile_staged": staged, "pairs": pairs}
+
+
+def porous_box_single(n=128, storage="fp16s", iters=24) -> dict:
+    import torch
+
+    lat = Lattice("d3q19", n, n, n, precision="fp32", storage=storage)
+    lat.set_flags(cases.porous_channel_d3q19(n, n, n, p=0.08, band=2, seed=1))
+    lat.SetSetting("nu", 0.02)
+    lat.SetSetting("ForceX", 1e-5)
+    lat.Init()
+    lat.Iterate(iters)
+    torch.cuda.synchronize()
+    path = lat.launch_path()
+    lat.close()
+    return {"workload": f"single lattice, d3q19 porous box {n}^3, {storage}", "iterations": iters, "path": path}
+
+
+def main(argv=None):
+    import argparse
+
+    p = argparse.ArgumentParser(description="profiling workloads (one JSON line)")
+    p.add_argument("what", choices=["porous-box-batch", "porous-box-single"])
+    p.add_argument("--n", type=int, default=128)
+    p.add_argument("--storage", default="fp16s")
+    p.add_argument("--no-tma", action="store_true")
+    a = p.parse_args(argv)
+    if a.what == "porous-box-batch":
+        r = porous_box_batch(a.n, a.storage, use_tma=not a.no_tma)
+    else:
+        r = porous_box_single(a.n, a.storage)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()
