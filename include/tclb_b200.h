@@ -264,9 +264,14 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    tclb_batch_sync. TCLB_BATCH_SHORT_TILES (on by default) halves the tile height, down to the
    block's thread rows, while the live cases would give fewer tiles than two
    waves of resident blocks; off, tiles are always by rows high. get_paths
-   gives the flags that are enabled and apply to the current launch shape
-   (TCLB_LAUNCH_TMA: to at least one live case). No TCLB counterpart. */
+   TCLB_BATCH_GLOBALS_AT_END (off by default) computes a case's Globals only
+   in the replay where it finishes (tclb_batch_get_globals then holds the
+   Globals of its last iteration once it is done, zeros before): the last
+   launch of the other replays runs the faster plain kernels for it.
+   get_paths gives the flags that are enabled and apply to the current launch
+   shape (TCLB_LAUNCH_TMA: to at least one live case). No TCLB counterpart. */
 #define TCLB_BATCH_SHORT_TILES 8
+#define TCLB_BATCH_GLOBALS_AT_END 16
 int tclb_batch_set_paths(tclb_batch_h b, int flags);
 int tclb_batch_get_paths(tclb_batch_h b, int* flags);
 

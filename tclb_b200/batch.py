@@ -157,13 +157,17 @@ class Batch:
         _check(self.lib.tclb_batch_get_launch(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
-    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True, use_tma: bool = True):
+    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True, use_tma: bool = True,
+                  globals_at_end: bool = False):
         """use_pairs: 16-bit storage lets plain launches update two nodes per
         thread when the tile shape allows it. short_tiles: lower the tile
         height while the live cases give too few tiles to fill the GPU.
         use_tma: 16-bit cases whose rows fit one TMA box take the tile-staged
-        kernel. All on by default."""
-        flags = (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if short_tiles else 0)
+        kernel. These three are on by default. globals_at_end (off by
+        default): a case's Globals are computed only in the replay where it
+        finishes (globals() holds them once it is done)."""
+        flags = (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if short_tiles else 0) | \
+            (16 if globals_at_end else 0)
         _check(self.lib.tclb_batch_set_paths(self._h, flags))
 
     def _paths(self) -> int:
@@ -243,11 +247,13 @@ K_CANDIDATES = [1, 4, 16, 64]
 
 
 def autotune(model, specs: Sequence[CaseSpec], precision="fp32", storage="same", tiles=TILE_CANDIDATES,
-             ks=K_CANDIDATES, trial_iters: int = 64, budget_bytes: int = 16 << 30) -> dict:
+             ks=K_CANDIDATES, trial_iters: int = 64, budget_bytes: int = 16 << 30, globals_at_end=False) -> dict:
     """Pick the tile shape and iterations per launch that maximise node updates
     per second on a scratch batch holding the given cases (the caller's cases
-    are not advanced). Returns {"bx","by","K","mlups","table"}."""
+    are not advanced), with the Globals mode the caller will use. Returns
+    {"bx","by","K","mlups","table"}."""
     b = Batch(model, precision, storage, budget_bytes=budget_bytes, max_cases=max(1, len(specs)))
+    b.set_paths(globals_at_end=globals_at_end)
     big = 1 << 30
     try:
         for s in specs:

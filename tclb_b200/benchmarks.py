@@ -178,8 +178,9 @@ def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True)
         tuned = None
         if tune:
             sample = specs[:: max(1, len(specs) // 64)]
-            tuned = autotune("d2q9", sample, precision="fp32", storage=st, trial_iters=64)
+            tuned = autotune("d2q9", sample, precision="fp32", storage=st, trial_iters=64, globals_at_end=True)
         b = Batch("d2q9", "fp32", storage=st, budget_bytes=100 << 30, max_cases=n_cases)
+        b.set_paths(globals_at_end=True)  # Globals of each case's last iteration only
         if tuned:
             b.set_launch(tuned["bx"], tuned["by"], tuned["K"])
         t_add = time.perf_counter()

@@ -59,14 +59,16 @@ struct BatchImpl {
   // (grid ga, bx threads per row).
   // group: the settings shared by the staged cases (models with the packed
   // collision; see tclb_batch::group)
+  // plain_last: launch K-1 also runs the plain kernels, for the cases that
+  // compute no Globals in this replay (TCLB_BATCH_GLOBALS_AT_END)
   void (*iterate)(const LaunchTables&, int k, int K, dim3 gp, dim3 ga, int tma_grid, const double* group, int bx,
-                  int by, int form, cudaStream_t);
+                  int by, int form, bool plain_last, cudaStream_t);
   // resident blocks of the tile-staged kernel on the device (it also sets the
   // kernel's shared-memory limit); 0 without one
   int (*tma_grid)(int sms);
   // the derived constants k of a case from its settings (host, in real_t)
   void (*derive)(BatchCase&);
-  void (*clear)(BatchCase*, int, cudaStream_t);
+  void (*clear)(BatchCase*, int n, int K, cudaStream_t);
   void (*init)(const BatchCase&, const void* dst, cudaStream_t, int bx, int by);
   void (*quantity)(const BatchCase&, int parity, int q, int vec, double scale, void* out, cudaStream_t);
   int (*blocks_per_sm)(int threads);
@@ -104,14 +106,14 @@ struct BL {
   static constexpr bool pairs = sizeof(typename St::T) == 2;  // 16-bit storage
   static size_t tma_smem() { return 128 + (size_t)tma_stages<M>() * (M::Q + 1) * TMA_TILE * 2; }
   static void iterate(const LaunchTables& L, int k, int K, dim3 gp, dim3 ga, int tma_grid, const double* group,
-                      int bx, int by, int form, cudaStream_t s) {
+                      int bx, int by, int form, bool plain_last, cudaStream_t s) {
     const dim3 b(bx, block_rows(bx, by, 256));
     const BatchCase* c = L.cases;
     const BatchTile* t = L.tiles;
-    if (k == K - 1) {  // every case's last iteration of the replay: Globals, all tiles
+    if (k == K - 1) {  // every case's last iteration of the replay: the Globals variant, all tiles
       if (form == FORM_PERSISTENT) k_iterate_batch<M, R, St, true><<<gp, b, 0, s>>>(c, t, L.ntiles + 1, k, K);
       else k_iterate_batch_tile<M, R, St, true><<<ga, b, 0, s>>>(c, t, L.ntiles + 1, k, K);
-      return;
+      if (!plain_last) return;
     }
     if constexpr (pairs) {
       if (tma_grid > 0) {
@@ -167,8 +169,8 @@ struct BL {
     }
     return n;
   }
-  static void clear(BatchCase* c, int n, cudaStream_t s) {
-    if (n > 0) k_batch_clear_globals<M::NG><<<n, 32, 0, s>>>(c, n);
+  static void clear(BatchCase* c, int n, int K, cudaStream_t s) {
+    if (n > 0) k_batch_clear_globals<M::NG><<<n, 32, 0, s>>>(c, n, K);
   }
   static void init(const BatchCase& C, const void* dst, cudaStream_t s, int bx, int by) {
     auto a = args_of<M, R>(C, nullptr, const_cast<void*>(dst));
@@ -470,10 +472,11 @@ int ensure_graph(tclb_batch* B) {
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   const int n = (int)B->cases.size();
-  B->I->clear(B->d_cases, n, B->stream);
+  B->I->clear(B->d_cases, n, B->K, B->stream);
   for (int k = 0; k < B->K; k++)
     B->I->iterate(L, k, B->K, dim3(B->grid_blocks), dim3(grid_all), has_tma ? B->tma_grid : 0,
-                  B->group.empty() ? nullptr : B->group.data(), B->bx, B->by, form, B->stream);
+                  B->group.empty() ? nullptr : B->group.data(), B->bx, B->by, form,
+                  (B->paths & TCLB_BATCH_GLOBALS_AT_END) != 0, B->stream);
   if (n > 0) {
     k_batch_advance<<<(n + 127) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->K);
     k_batch_status<<<(n + 128) / 128, 128, 0, B->stream>>>(B->d_cases, n, B->d_err, B->d_status);
@@ -628,6 +631,7 @@ int tclb_batch_add_case(tclb_batch_h B, int nx, int ny, int nz, const uint16_t* 
   C.counter = 0;
   C.remaining = niter;
   C.active = 1;
+  C.glob_end = (B->paths & TCLB_BATCH_GLOBALS_AT_END) ? 1 : 0;
   BatchTmaMaps maps;  // host copy of the tensor maps, uploaded below
   if (L.maps) {
     const int R = tma_rows_for(B->elem, nx, ny);
@@ -717,9 +721,19 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
 
 int tclb_batch_set_paths(tclb_batch_h B, int flags) {
   CHECK_B(B);
-  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES))
+  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES | TCLB_BATCH_GLOBALS_AT_END))
     return bfail(TCLB_ERR_ARG, "unknown path flags");
   if (flags != B->paths) B->tiles_dirty = true;
+  if ((flags ^ B->paths) & TCLB_BATCH_GLOBALS_AT_END) {  // the case descriptors carry the Globals mode
+    BCK(cudaStreamSynchronize(B->stream));
+    for (size_t s = 0; s < B->cases.size(); s++) {
+      if (!B->used_slot[s]) continue;
+      B->cases[s].glob_end = (flags & TCLB_BATCH_GLOBALS_AT_END) ? 1 : 0;
+      int rc = upload_case(B, (int)s);
+      if (rc) return rc;
+    }
+    BCK(cudaStreamSynchronize(B->stream));
+  }
   B->paths = flags;
   B->graph_key[0] = -1;
   return TCLB_OK;
@@ -733,7 +747,7 @@ int tclb_batch_get_paths(tclb_batch_h B, int* flags) {
   for (size_t s = 0; s < B->cases.size(); s++) any_staged |= live(B, s) && staged(B, B->cases[s]);
   if (flags)
     *flags = (pair_form(B) ? TCLB_LAUNCH_PAIRS : 0) | (any_staged ? TCLB_LAUNCH_TMA : 0) |
-             (B->paths & TCLB_BATCH_SHORT_TILES);
+             (B->paths & (TCLB_BATCH_SHORT_TILES | TCLB_BATCH_GLOBALS_AT_END));
   return TCLB_OK;
 }
 

@@ -51,6 +51,7 @@ struct BatchCase {
   int counter;    // iterations done
   int remaining;  // iterations left
   int active;
+  int glob_end;               // 1: Globals only in the replay where the case finishes
   int tma_rows;               // rows per staged tile; 0: the case is not staged
   const BatchTmaMaps* maps;   // with tma_rows > 0
   double s[BATCH_MAX_SET];
@@ -87,14 +88,22 @@ struct GroupArgs {
   const R* zone;
 };
 
-// Whether case C runs at launch k of a replay of K, and the A/B parity of
-// that iteration: a case with d iterations left runs launches K-d .. K-1.
-__device__ __forceinline__ bool case_runs(const BatchCase& C, int k, int K, int& parity) {
+// Whether case C computes Globals in this replay (of K launches): in every
+// replay, or with glob_end only in the one where it finishes.
+__device__ __forceinline__ bool case_globals(const BatchCase& C, int K) { return !C.glob_end || C.remaining <= K; }
+
+// Whether case C runs at launch k of a replay of K in a kernel of the
+// Globals variant (G) or a plain one, and the A/B parity of that iteration:
+// a case with d iterations left runs launches K-d .. K-1. Launch K-1 is its
+// last iteration of the replay: the Globals variant takes the cases that
+// compute Globals in this replay, the plain kernels the others.
+__device__ __forceinline__ bool case_runs(const BatchCase& C, int k, int K, bool G, int& parity) {
   const int remaining = C.remaining;
   const int d = remaining < K ? remaining : K;
   const int first = K - d;
   parity = (C.counter + (k - first)) & 1;
-  return C.active && d > 0 && k >= first;
+  const bool on = C.active && d > 0 && k >= first;
+  return k == K - 1 ? on && G == case_globals(C, K) : on && !G;
 }
 
 // The node-update arguments of case C at the given parity (the derived
@@ -137,7 +146,7 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
         slot = tile.slot;
         const BatchCase& C = cases[slot];
         int parity;
-        skip = !case_runs(C, k, K, parity);
+        skip = !case_runs(C, k, K, G, parity);
         case_args<M, R>(C, parity, a);
       }
       if (skip) continue;
@@ -163,7 +172,7 @@ __global__ void __launch_bounds__(256) k_iterate_batch(const BatchCase* __restri
 
 // The arguments of tile t at launch k of a replay of K; false if the block
 // has nothing to do (past the live tiles, or the case idle at this launch).
-template <class M, class R>
+template <class M, class R, bool G>
 __device__ __forceinline__ bool batch_tile_args(const BatchCase* __restrict__ cases,
                                                 const BatchTile* __restrict__ tiles, const int* __restrict__ ntiles_p,
                                                 int k, int K, BatchTile& tile, Args<R, M::NSET>& a) {
@@ -172,7 +181,7 @@ __device__ __forceinline__ bool batch_tile_args(const BatchCase* __restrict__ ca
   tile = tiles[t];
   const BatchCase& C = cases[tile.slot];
   int parity;
-  if (!case_runs(C, k, K, parity)) return false;
+  if (!case_runs(C, k, K, G, parity)) return false;
   case_args<M, R>(C, parity, a);
   return true;
 }
@@ -186,7 +195,7 @@ __global__ void __launch_bounds__(256, (G || sizeof(R) == 8) ? 1 : M::BATCH_MIN_
                          const int* __restrict__ ntiles_p, int k, int K) {
   BatchTile tile;
   Args<R, M::NSET> a;
-  if (!batch_tile_args<M, R>(cases, tiles, ntiles_p, k, K, tile, a)) return;
+  if (!batch_tile_args<M, R, G>(cases, tiles, ntiles_p, k, K, tile, a)) return;
   const int x = tile.x0 + threadIdx.x, z = tile.z;
   const int y_end = min(tile.y0 + tile.h, a.ny);
   using T = typename St::T;
@@ -218,7 +227,7 @@ __global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
                          const int* __restrict__ ntiles_p, int k, int K) {
   BatchTile tile;
   Args<R, M::NSET> a;
-  if (!batch_tile_args<M, R>(cases, tiles, ntiles_p, k, K, tile, a)) return;
+  if (!batch_tile_args<M, R, false>(cases, tiles, ntiles_p, k, K, tile, a)) return;
   using T = typename St::T;
   const StrideAddr<T> P{static_cast<const T*>(a.src), static_cast<T*>(a.dst), a.stride};
   const int z = tile.z;
@@ -288,7 +297,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       if (tile.slot != slot) {  // the case's run predicate, parity and shape hold for the launch
         slot = tile.slot;
         const BatchCase& C = cases[slot];
-        run = case_runs(C, k, K, parity);
+        run = case_runs(C, k, K, false, parity);
         nx = C.nx;
         ny = C.ny;
         nz = C.nz;
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       slot = tile.slot;
       const BatchCase& C = cases[slot];
       int parity;
-      run = case_runs(C, k, K, parity);
+      run = case_runs(C, k, K, false, parity);
       __syncwarp();
       if constexpr (!M::has_bulk) {
         if (lane == 0) case_args<M, R>(C, parity, a);
@@ -406,11 +415,12 @@ __global__ void k_batch_advance(BatchCase* cases, int ncases, int K) {
   cases[c].remaining = r - d;
 }
 
-// Clear the Globals of every case at the start of a replay.
+// Clear, at the start of a replay, the Globals of every case that computes
+// them in this replay.
 template <int NG>
-__global__ void k_batch_clear_globals(BatchCase* cases, int ncases) {
+__global__ void k_batch_clear_globals(BatchCase* cases, int ncases, int K) {
   const int c = blockIdx.x;
-  if (c >= ncases || !cases[c].active || cases[c].remaining <= 0) return;
+  if (c >= ncases || !cases[c].active || cases[c].remaining <= 0 || !case_globals(cases[c], K)) return;
   for (int i = threadIdx.x; i < NG; i += blockDim.x) cases[c].glob[i] = 0.0;
 }
 

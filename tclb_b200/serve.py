@@ -57,6 +57,7 @@ class Server:
         for m in models:
             # each batch may use the whole budget; the server enforces the sum
             b = Batch(m, precision, storage, budget_bytes=self.budget, max_cases=max_cases)
+            b.set_paths(globals_at_end=True)  # a result's Globals are read when it is done
             if launch and m in launch:
                 b.set_launch(*launch[m])
             if m in high_priority:  # small cases: their blocks go first

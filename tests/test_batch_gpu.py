@@ -324,3 +324,37 @@ def test_batch_tile_staged_late_admission_and_retire():
         a.run_to_completion()
         assert np.array_equal(a.quantity(c, "U"), u)
         a.close()
+
+
+@pytest.mark.parametrize("model,storage,shapes", [
+    ("d3q19", "fp16s", [(4, 16, 64), (3, 8, 96), (2, 12, 128)]),
+    ("d2q9", "same", [(1, 24, 64), (1, 16, 96)]),
+])
+def test_globals_at_end(model, storage, shapes):
+    """With Globals only in each case's finishing replay, the last launch of
+    the other replays takes the plain kernels. In FP32 that is the same node
+    update: fields and final Globals equal those of the default mode. With
+    16-bit storage the plain kernels are the two-node ones, whose float
+    rounding may flip a 16-bit value (the 1e-3 bar of the two-node path).
+    Before a case finishes its Globals are zero."""
+    specs = [_random_case(model, sh, seed=61 + i, niter=n) for i, (sh, n) in enumerate(zip(shapes, (17, 9, 30)))]
+    out = []
+    for at_end in (False, True):
+        b = Batch(model, "fp32", storage=storage, budget_bytes=1 << 30)
+        b.set_launch(64, 8, 4)
+        b.set_paths(globals_at_end=at_end)
+        ids = [b.add_case(s) for s in specs]
+        b.step()
+        b.sync()
+        mid = b.globals(ids[-1])  # 30 iterations: not finished after one replay
+        b.run_to_completion()
+        out.append((mid, [(b.quantity(c, "U"), b.globals(c)) for c in ids]))
+        b.close()
+    (mid0, r0), (mid1, r1) = out
+    assert np.any(mid0 != 0) and not np.any(mid1 != 0)
+    for (u0, g0), (u1, g1) in zip(r0, r1):
+        if storage == "same":
+            assert np.array_equal(u0, u1) and np.array_equal(g0, g1)
+        else:
+            assert rel_l2(u1, u0) < 1e-3
+            assert np.allclose(g1, g0, rtol=1e-2, atol=1e-3 * np.abs(g0).max())
