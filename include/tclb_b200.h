@@ -261,16 +261,19 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    dividing ny) through the tile-staged kernel, tensor maps kept with the case;
    the other cases take the pair or one-node form. A staging wait that runs
    out (about a second) is reported as TCLB_ERR_CUDA by the next
-   tclb_batch_sync. TCLB_BATCH_SHORT_TILES (on by default) halves the tile height, down to the
-   block's thread rows, while the live cases would give fewer tiles than two
-   waves of resident blocks; off, tiles are always by rows high. get_paths
+   tclb_batch_sync. TCLB_BATCH_ADAPTIVE (on by default) fits the launches to
+   the live work: it halves the tile height, down to the block's thread rows,
+   while the live cases would give fewer tiles than two waves of resident
+   blocks, and leaves the tile-staged kernel out while the staged cases give
+   fewer than 8 tiles per resident block (its pipeline start would dominate);
+   off, tiles are always by rows high and every case that fits is staged.
    TCLB_BATCH_GLOBALS_AT_END (off by default) computes a case's Globals only
    in the replay where it finishes (tclb_batch_get_globals then holds the
    Globals of its last iteration once it is done, zeros before): the last
    launch of the other replays runs the faster plain kernels for it.
    get_paths gives the flags that are enabled and apply to the current launch
    shape (TCLB_LAUNCH_TMA: to at least one live case). No TCLB counterpart. */
-#define TCLB_BATCH_SHORT_TILES 8
+#define TCLB_BATCH_ADAPTIVE 8
 #define TCLB_BATCH_GLOBALS_AT_END 16
 int tclb_batch_set_paths(tclb_batch_h b, int flags);
 int tclb_batch_get_paths(tclb_batch_h b, int* flags);

@@ -157,16 +157,16 @@ class Batch:
         _check(self.lib.tclb_batch_get_launch(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
-    def set_paths(self, use_pairs: bool = True, short_tiles: bool = True, use_tma: bool = True,
+    def set_paths(self, use_pairs: bool = True, adaptive: bool = True, use_tma: bool = True,
                   globals_at_end: bool = False):
         """use_pairs: 16-bit storage lets plain launches update two nodes per
-        thread when the tile shape allows it. short_tiles: lower the tile
-        height while the live cases give too few tiles to fill the GPU.
-        use_tma: 16-bit cases whose rows fit one TMA box take the tile-staged
-        kernel. These three are on by default. globals_at_end (off by
-        default): a case's Globals are computed only in the replay where it
-        finishes (globals() holds them once it is done)."""
-        flags = (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if short_tiles else 0) | \
+        thread when the tile shape allows it. use_tma: 16-bit cases whose rows
+        fit one TMA box take the tile-staged kernel. adaptive: lower the tile
+        height, and leave the tile-staged kernel out, while the live cases give
+        too few tiles to fill the GPU. These three are on by default.
+        globals_at_end (off by default): a case's Globals are computed only in
+        the replay where it finishes (globals() holds them once it is done)."""
+        flags = (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if adaptive else 0) | \
             (16 if globals_at_end else 0)
         _check(self.lib.tclb_batch_set_paths(self._h, flags))
 

@@ -287,6 +287,7 @@ struct tclb_batch {
   // cases with these settings are staged (the others take the pair kernel).
   // Chosen when the tile table is rebuilt: kept while a live case has them.
   std::vector<double> group;
+  bool staging = false;  // the staged kernel runs (update_staging)
   int status_n = -1;  // cases in the status read back by the last step (its error word follows)
   cudaGraphExec_t graph = nullptr;
   cudaGraph_t graph_src = nullptr;          // kept: its nodes address the instantiated graph
@@ -294,7 +295,7 @@ struct tclb_batch {
   std::vector<cudaGraphNode_t> glob_nodes;   // the Globals launch
   int graph_grid[2] = {0, 0};                // their grids in the instantiated graph
   int graph_key[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-  int paths = TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES;  // tclb_batch_set_paths
+  int paths = TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_ADAPTIVE;  // tclb_batch_set_paths
 };
 
 namespace {
@@ -320,12 +321,14 @@ bool in_group(const tclb_batch* B, const BatchCase& C) {
   return true;
 }
 
-// Plain launches of this case take the tile-staged kernel: staging enabled,
-// one block per tile, the case fits it (tensor maps were made) and belongs
-// to the staged group.
-bool staged(const tclb_batch* B, const BatchCase& C) {
+// The case could take the tile-staged kernel: staging enabled, one block per
+// tile, the case fits it (tensor maps were made) and belongs to the group.
+bool stageable(const tclb_batch* B, const BatchCase& C) {
   return (B->paths & TCLB_LAUNCH_TMA) && B->user_grid == 0 && C.tma_rows > 0 && B->tma_grid > 0 && in_group(B, C);
 }
+
+// Plain launches of this case take the tile-staged kernel (see update_staging).
+bool staged(const tclb_batch* B, const BatchCase& C) { return B->staging && stageable(B, C); }
 
 bool live(const tclb_batch* B, size_t s) {
   return B->used_slot[s] && B->cases[s].active && B->h_status[s].y > 0;  // finished cases get no tiles
@@ -337,7 +340,7 @@ bool live(const tclb_batch* B, size_t s) {
 int tile_height(const tclb_batch* B) {
   int floor_h = block_rows(B->bx, B->by, 256);
   if (pair_form(B)) floor_h = std::max(floor_h, block_rows(B->bx / 2, B->by, B->I->pair_threads));
-  if (!(B->paths & TCLB_BATCH_SHORT_TILES)) return B->by;
+  if (!(B->paths & TCLB_BATCH_ADAPTIVE)) return B->by;
   int per_sm = B->I->blocks_per_sm(B->bx * floor_h);
   if (per_sm < 1) per_sm = std::max(1, 2048 / (B->bx * floor_h));
   const size_t want = (size_t)2 * B->sms * per_sm;
@@ -385,9 +388,24 @@ void choose_group(tclb_batch* B) {
   }
 }
 
-int rebuild_tiles(tclb_batch* B) {
+// Staging on while the stageable live cases give at least 8 tiles per
+// resident block of the persistent staged kernel (with TCLB_BATCH_ADAPTIVE):
+// with fewer, its per-launch pipeline start costs more than it saves.
+void update_staging(tclb_batch* B) {
   if (B->tma_grid < 0) B->tma_grid = B->I->tma_grid(B->sms);
   choose_group(B);
+  size_t n = 0;
+  for (size_t s = 0; s < B->cases.size(); s++) {
+    const BatchCase& C = B->cases[s];
+    if (live(B, s) && stageable(B, C)) n += (size_t)C.nz * (C.ny / C.tma_rows);
+  }
+  const bool on = n > 0 && (!(B->paths & TCLB_BATCH_ADAPTIVE) || n >= (size_t)8 * B->tma_grid);
+  if (on != B->staging) B->tiles_dirty = true;
+  B->staging = on;
+}
+
+int rebuild_tiles(tclb_batch* B) {
+  update_staging(B);
   std::vector<BatchTile> t;
   std::vector<BatchTmaTile> tt;
   const int h = tile_height(B);
@@ -721,7 +739,7 @@ int tclb_batch_set_launch(tclb_batch_h B, int bx, int by, int iters_per_launch, 
 
 int tclb_batch_set_paths(tclb_batch_h B, int flags) {
   CHECK_B(B);
-  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_SHORT_TILES | TCLB_BATCH_GLOBALS_AT_END))
+  if (flags & ~(TCLB_LAUNCH_PAIRS | TCLB_LAUNCH_TMA | TCLB_BATCH_ADAPTIVE | TCLB_BATCH_GLOBALS_AT_END))
     return bfail(TCLB_ERR_ARG, "unknown path flags");
   if (flags != B->paths) B->tiles_dirty = true;
   if ((flags ^ B->paths) & TCLB_BATCH_GLOBALS_AT_END) {  // the case descriptors carry the Globals mode
@@ -741,13 +759,12 @@ int tclb_batch_set_paths(tclb_batch_h B, int flags) {
 
 int tclb_batch_get_paths(tclb_batch_h B, int* flags) {
   CHECK_B(B);
-  if (B->tma_grid < 0) B->tma_grid = B->I->tma_grid(B->sms);
-  choose_group(B);
+  update_staging(B);
   bool any_staged = false;
   for (size_t s = 0; s < B->cases.size(); s++) any_staged |= live(B, s) && staged(B, B->cases[s]);
   if (flags)
     *flags = (pair_form(B) ? TCLB_LAUNCH_PAIRS : 0) | (any_staged ? TCLB_LAUNCH_TMA : 0) |
-             (B->paths & (TCLB_BATCH_SHORT_TILES | TCLB_BATCH_GLOBALS_AT_END));
+             (B->paths & (TCLB_BATCH_ADAPTIVE | TCLB_BATCH_GLOBALS_AT_END));
   return TCLB_OK;
 }
 

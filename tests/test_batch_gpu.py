@@ -234,7 +234,7 @@ def test_tall_tiles_walk_rows(storage, short, tall):
     for bx, by in (short, tall):
         b = Batch("d3q19", "fp32", storage=storage, budget_bytes=1 << 30)
         b.set_launch(bx, by, 3)
-        b.set_paths(short_tiles=False)  # these few small cases would get short tiles
+        b.set_paths(adaptive=False)  # these few small cases would get short tiles
         ids = [b.add_case(s) for s in specs]
         b.step()
         want = sum(s.shape[0] * -(-s.shape[1] // by) * -(-s.shape[2] // bx) for s in specs)
@@ -255,7 +255,7 @@ def test_short_tiles_when_few():
     for short in (True, False):
         b = Batch("d2q9", "fp32", budget_bytes=1 << 28)
         b.set_launch(64, 64, 5)
-        b.set_paths(short_tiles=short)
+        b.set_paths(adaptive=short)
         c = b.add_case(spec)
         b.step()
         res.append((b.info()["tiles"], b.quantity(c, "U")))
@@ -288,7 +288,7 @@ def test_batch_tile_staged_matches_pairs_bit_for_bit(model, storage):
     for tma in (True, False):
         b = Batch(model, "fp32", storage=storage, budget_bytes=1 << 30)
         b.set_launch(64, 4, 4)  # K does not divide the iteration count
-        b.set_paths(use_tma=tma)
+        b.set_paths(use_tma=tma, adaptive=False)  # stage these small cases too
         ids = [b.add_case(s) for s in specs]
         assert b.uses_tma() == tma and b.uses_pairs()
         b.run_to_completion()
@@ -308,6 +308,7 @@ def test_batch_tile_staged_late_admission_and_retire():
              for i, (sh, n) in enumerate([((4, 16, 64), 13), ((3, 8, 96), 6), ((2, 12, 128), 20)])]
     b = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=1 << 30)
     b.set_launch(64, 8, 5)
+    b.set_paths(adaptive=False)  # stage these small cases too
     c0 = b.add_case(specs[0])
     c1 = b.add_case(specs[1])
     b.step()
@@ -358,3 +359,16 @@ def test_globals_at_end(model, storage, shapes):
         else:
             assert rel_l2(u1, u0) < 1e-3
             assert np.allclose(g1, g0, rtol=1e-2, atol=1e-3 * np.abs(g0).max())
+
+
+def test_staging_needs_enough_tiles():
+    """Adaptive: a small stageable case alone runs the register kernels (too
+    few tiles for the persistent staged kernel); a large one is staged."""
+    def uses_tma(n):
+        b = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=4 << 30)
+        b.set_launch(64, 16, 4)
+        b.add_case(CaseSpec(cases.porous_channel_d3q19(n, n, n, p=0.05, band=2, seed=3), {"nu": 0.02}, {}, 4))
+        r = b.uses_tma()
+        b.close()
+        return r
+    assert not uses_tma(64) and uses_tma(128)
