@@ -3,7 +3,8 @@
 // counterpart in the reference, which runs one lattice per process).
 //
 // Memory: each case is one allocation from a stream-ordered CUDA memory pool
-// owned by the batch (two snapshots, node types, zonal settings, Globals), so
+// owned by the batch (two snapshots, node types, zonal settings, Globals and,
+// for a case the tile-staged kernel can take, its tensor maps), so
 // admitting and retiring cases never synchronises the device. A byte budget
 // bounds the sum of case footprints; admission beyond it is refused.
 #include <cuda_runtime.h>

@@ -8,7 +8,9 @@
 // the SMs through the hardware block scheduler; a persistent grid walking
 // the table with a grid stride (k_iterate_batch) is the alternative, slower
 // on mixed sizes. The physics is the per-model node update of
-// lbm_kernels.cuh, unchanged.
+// lbm_kernels.cuh, unchanged. With 16-bit storage the plain launches take
+// the two-nodes-per-thread update (k_iterate_batch_pair) and, for cases whose
+// rows fit one TMA box, the tile-staged pipeline (k_iterate_batch_tma).
 //
 // A tile is a bx x by block of nodes of one z plane of one case. With nx a
 // multiple of 32 (TCLB's padding) a tile width of 32 leaves no thread idle on
@@ -21,7 +23,9 @@
 // A launch is iteration k (0-based) of a replay of K iterations. A case with
 // d = min(remaining, K) iterations to do in this replay runs the last d
 // launches, k = K-d .. K-1, so every case's last iteration of a replay is
-// launch K-1: that launch alone is the Globals variant, and the plain
+// launch K-1: that launch alone is the Globals variant (for the cases that
+// compute Globals in this replay: every replay, or with glob_end only the
+// finishing one; the others take the plain kernels at K-1 too), and the plain
 // launches carry no Globals code (the register count of the one-lattice
 // kernel, not of both paths). Its A/B parity at launch k is
 // (counter + k - (K - d)) & 1. The counters advance only in k_batch_advance
