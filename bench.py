@@ -62,6 +62,8 @@ def parse():
                         "applies, else two nodes per thread), tma, pairs, one (one node per thread)")
     p.add_argument("--config", type=int, default=2,
                    help="2 = the headline Taylor-Green line; 1, 3, 4, 5 = the other configurations (one JSON line)")
+    p.add_argument("--accuracy", action="store_true",
+                   help="with --config 2: velocity, energy and enstrophy errors of each storage against FP64")
     return p.parse_args()
 
 
@@ -375,8 +377,11 @@ def run_config(args):
     from tclb_b200 import benchmarks as BM
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    fn = {1: BM.config1, 3: BM.config3, 4: BM.config4, 5: BM.config5}[args.config]
-    res = fn(rate=args.rate) if args.config == 5 else fn()
+    if args.config == 2:  # --accuracy
+        res = BM.config2_accuracy(n=args.n)
+    else:
+        fn = {1: BM.config1, 3: BM.config3, 4: BM.config4, 5: BM.config5}[args.config]
+        res = fn(rate=args.rate) if args.config == 5 else fn()
     print(json.dumps({"metric": METRIC, "unit": UNIT, "config_id": args.config, "data": "synthetic", **res}),
           flush=True)
     return 0
@@ -386,7 +391,7 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.config != 2:
+    if args.config != 2 or args.accuracy:
         return run_config(args)
     return run_ours(args)
 

@@ -252,6 +252,47 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150)
 
 
 # ---------------------------------------------------------------------------
+# Configuration 2 accuracy: the Taylor-Green vortex of the throughput lines
+# run in each storage next to an FP64 run of the same case; relative L2 error
+# of the velocity field and relative errors of the kinetic energy and
+# enstrophy after the given iterations.
+# ---------------------------------------------------------------------------
+TGV_NU = {"d3q27_cumulant": 1e-3, "d3q19": 1e-2}
+
+
+def config2_accuracy(models=("d3q27_cumulant", "d3q19"), n=256, iterations=2000,
+                     storages=("fp32", "fp16s", "bf16s")) -> dict:
+    out = {"config": f"2 (accuracy): Taylor-Green vortex {n}^3, u0 = 0.05, {iterations} iterations, each storage "
+                     "against an FP64 run of the same case", "runs": {}}
+    for model in models:
+        res, ref_u, ref_ee = {}, None, None
+        for st in ("fp64",) + tuple(storages):
+            prec = "fp64" if st == "fp64" else "fp32"
+            storage = "same" if st in ("fp64", "fp32") else st
+            lat = Lattice(model, n, n, n, precision=prec, storage=storage)
+            lat.set_flags(cases.tgv_flags(model, n))
+            lat.SetSetting("nu", TGV_NU[model])
+            rho, u = cases.tgv_fields(n, u0=0.05, dtype=lat.real)
+            lat.init_equilibrium(rho, u)
+            lat.Iterate(iterations)
+            u = lat.GetQuantity("U").astype(np.float64)
+            ee = lat.energy_enstrophy()
+            path = lat.launch_path()
+            lat.close()
+            if st == "fp64":
+                ref_u, ref_ee = u, ee
+                res[st] = {"kinetic_energy": ee[0], "enstrophy": ee[1]}
+                continue
+            res[st] = {"u_rel_l2_vs_fp64": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u)),
+                       "energy_rel_err": abs(ee[0] - ref_ee[0]) / abs(ref_ee[0]),
+                       "enstrophy_rel_err": abs(ee[1] - ref_ee[1]) / abs(ref_ee[1]),
+                       "path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")}
+            del u
+        out["runs"][model] = res
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Profiling workloads: one porous d3q19 box (p = 0.08, 2-node wall band, seed
 # 1), n^3 nodes, advanced through a batch (its kernel path chosen by the
 # batch's paths) or through a single lattice. Small enough for an ncu capture.
