@@ -376,14 +376,24 @@ def run_config(args):
 
     from tclb_b200 import benchmarks as BM
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    if args.config == 2:  # --accuracy
+    from tclb_b200.replicas import Replicas
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if args.config in (4, 5):
+        # independent cases / requests shared out over the ranks, no exchange
+        reps = Replicas("nccl" if world > 1 else "gloo")
+        res = BM.config4(reps=reps) if args.config == 4 else BM.config5(rate=args.rate, reps=reps)
+        reps.close()
+    elif rank != 0:  # one case: rank 0 alone runs it
+        return 0
+    elif args.config == 2:  # --accuracy
         res = BM.config2_accuracy(n=args.n)
     else:
-        fn = {1: BM.config1, 3: BM.config3, 4: BM.config4, 5: BM.config5}[args.config]
-        res = fn(rate=args.rate) if args.config == 5 else fn()
-    print(json.dumps({"metric": METRIC, "unit": UNIT, "config_id": args.config, "data": "synthetic", **res}),
-          flush=True)
+        res = {1: BM.config1, 3: BM.config3}[args.config]()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "unit": UNIT, "config_id": args.config, "data": "synthetic", **res}),
+              flush=True)
     return 0
 
 

@@ -168,18 +168,39 @@ def single_large_mlups(model="d2q9", shape=(1, 1024, 4096), precision="fp32", st
     return n * iters / t / 1e6
 
 
-def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True) -> dict:
+def aggregate_batch(reps, updates: float, seconds: float, ncases: int, single: float) -> dict:
+    """Whole-job figures of a batch run whose cases are shared out over the
+    ranks: the work of all ranks over the slowest rank's time, and the
+    fraction of N times the single-large-case rate (the ranks' mean)."""
+    t = reps.reduce_max(seconds)
+    u = reps.reduce_sum(updates)
+    c = reps.reduce_sum(ncases)
+    single_mean = reps.reduce_sum(single) / reps.world
+    mlups = u / t / 1e6 if t > 0 else 0.0
+    return {"MLUPS": mlups, "cases_per_s": c / t if t > 0 else 0.0, "time_s": t,
+            "single_large_case_MLUPS": single_mean, "fraction_of_single": mlups / (reps.world * single_mean)}
+
+
+def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True, reps=None) -> dict:
+    """With reps over N > 1 ranks (one GPU each) the cases are shared out by
+    work (replicas.partition_cases), with no exchange between the ranks."""
+    from .replicas import Replicas, partition_cases
+
+    reps = reps or Replicas("gloo")
     specs, clamps = batch_specs(n_cases, iterations=iterations)
     nodes = sum(int(np.prod(s.shape)) for s in specs)
+    mine = partition_cases([float(np.prod(s.shape)) for s in specs], reps.world)[reps.rank]
+    specs = [specs[i] for i in mine]
+    my_nodes = sum(int(np.prod(s.shape)) for s in specs)
     out = {"config": f"4: {n_cases} d2q9 BGK-like cases, W log-uniform 64..2048 (H=W/4), one disc each, "
                      f"Ux=0.02, Re U[20,200], {iterations} iterations each, persistent graph-captured launches",
-           "nodes_total": nodes, "omega_clamps": clamps, "runs": {}}
+           "nodes_total": nodes, "omega_clamps": clamps, "gpus": reps.world, "runs": {}}
     for st in storages:
         tuned = None
         if tune:
             sample = specs[:: max(1, len(specs) // 64)]
             tuned = autotune("d2q9", sample, precision="fp32", storage=st, trial_iters=64, globals_at_end=True)
-        b = Batch("d2q9", "fp32", storage=st, budget_bytes=100 << 30, max_cases=n_cases)
+        b = Batch("d2q9", "fp32", storage=st, budget_bytes=100 << 30, max_cases=max(1, len(specs)))
         b.set_paths(globals_at_end=True)  # Globals of each case's last iteration only
         if tuned:
             b.set_launch(tuned["bx"], tuned["by"], tuned["K"])
@@ -187,14 +208,13 @@ def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True)
         ids = [b.add_case(s) for s in specs]
         t_add = time.perf_counter() - t_add
         b.sync()
+        reps.barrier()
         t0 = time.perf_counter()
         steps = b.run_to_completion()
         t = time.perf_counter() - t0
-        mlups = nodes * iterations / t / 1e6
         single = single_large_mlups(storage=st)
-        r = {"MLUPS": mlups, "cases_per_s": n_cases / t, "time_s": t, "replays": steps,
-             "admission_s": t_add, "single_large_case_MLUPS": single, "fraction_of_single": mlups / single,
-             "launch": dict(zip(("bx", "by", "K"), b.get_launch()))}
+        r = aggregate_batch(reps, float(my_nodes) * iterations, t, len(ids), single)
+        r.update({"replays": steps, "admission_s": t_add, "launch": dict(zip(("bx", "by", "K"), b.get_launch()))})
         if tuned:
             r["autotune_table"] = tuned["table"]
         out["runs"][st] = r
@@ -227,15 +247,45 @@ def serve_requests(n_requests=120, rate=6.0, seed=0, d3_edge=(64, 256), iters=(5
     return out
 
 
-def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150) -> dict:
+def aggregate_serving(reps, rep: dict, tts: list, updates: float, ideal_s: float) -> dict:
+    """Whole-job serving figures over the ranks (each serving its share of
+    the requests on its own GPU): requests and updates of all ranks over the
+    longest wall time, time-to-solution percentiles over all requests, and
+    the efficiency as the ideal single-large-case time of all served updates
+    over the GPU-seconds the servers had work in flight."""
+    parts = reps.gather({"tts": list(tts), "updates": float(updates), "ideal": float(ideal_s),
+                         "busy": float(rep["busy_s"]), "wall": float(rep["wall_s"]), "rounds": int(rep["rounds"]),
+                         "pending": int(rep["pending"])})
+    all_tts = np.array([t for p in parts for t in p["tts"]]) if any(p["tts"] for p in parts) else np.zeros(1)
+    n = sum(len(p["tts"]) for p in parts)
+    upd = sum(p["updates"] for p in parts)
+    busy = sum(p["busy"] for p in parts)
+    wall = max(p["wall"] for p in parts)
+    ideal = sum(p["ideal"] for p in parts)
+    return {"requests": n, "wall_s": wall, "cases_per_s": n / wall if wall else 0.0,
+            "mlups": upd / wall / 1e6 if wall else 0.0, "busy_s": busy,
+            "busy_mlups": upd / busy / 1e6 * reps.world if busy else 0.0,
+            "p50_s": float(np.percentile(all_tts, 50)), "p99_s": float(np.percentile(all_tts, 99)),
+            "rounds": sum(p["rounds"] for p in parts), "pending": sum(p["pending"] for p in parts),
+            "fraction_of_single": ideal / busy if busy else 0.0, "gpus": reps.world}
+
+
+def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150, reps=None) -> dict:
+    """With reps over N > 1 ranks the requests are dealt out round-robin in
+    arrival order (request i to rank i mod N), each rank serving its share on
+    its own GPU with no exchange; the figures are aggregated over the ranks."""
+    from .replicas import Replicas
+
+    reps = reps or Replicas("gloo")
     out = {"config": f"5: serving, Poisson arrivals (rate {rate}/s, seed 0), 70% d2q9 obstacle channels (config-4 "
                      "sizes), 30% d3q19 porous boxes (edge U[64,256], p U[0.02,0.15]), iterations U[500,5000], "
                      f"admission by footprint under {budget_gb} GB, resident lattices, continuous batching",
-           "runs": {}}
+           "gpus": reps.world, "runs": {}}
     for st in storages:
-        reqs = serve_requests(n_requests, rate)
+        reqs = serve_requests(n_requests, rate)[reps.rank::reps.world]
         srv = Server(("d2q9", "d3q19"), "fp32", st, budget_bytes=budget_gb << 30,
                      launch={"d2q9": (64, 64, 64), "d3q19": (64, 16, 16) if st == "same" else (64, 64, 16)})
+        reps.barrier()
         rep = srv.run(reqs)
         done = srv.done
         srv.close()
@@ -245,9 +295,10 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150)
         single = {"d2q9": single_large_mlups("d2q9", storage=st),
                   "d3q19": single_large_mlups("d3q19", (256, 256, 256), storage=st, iters=100)}
         t_ideal = sum(r.updates / (single[r.model] * 1e6) for r in done)
-        rep["single_large_case_MLUPS"] = single
-        rep["fraction_of_single"] = t_ideal / rep["busy_s"] if rep["busy_s"] else 0.0
-        out["runs"][st] = rep
+        agg = aggregate_serving(reps, rep, [r.finished - r.arrival for r in done], sum(r.updates for r in done),
+                                t_ideal)
+        agg["single_large_case_MLUPS"] = single
+        out["runs"][st] = agg
     return out
 
 

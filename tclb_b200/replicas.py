@@ -1,9 +1,10 @@
 """Replicas across GPUs: one independent lattice per rank, no data exchange.
 
 A single TCLB case is not sharded here (one GPU per case), so a run on N GPUs
-is N replicas (or N shares of independent batched cases). The only
-cross-rank steps are host coordination: a barrier around the timed region and
-reductions of the per-rank device times and work counts. The whole-job rate
+is N replicas, or N shares of independent batched cases (partition_cases,
+every case on exactly one rank). The only cross-rank steps are host
+coordination: a barrier around the timed region, reductions of the per-rank
+times and work counts, and a gather of per-case results. The whole-job rate
 is the work all ranks did divided by the slowest rank's time.
 
 The backend is "nccl" with CUDA tensors on GPUs and "gloo" with CPU tensors
@@ -15,6 +16,20 @@ from __future__ import annotations
 import datetime
 import os
 from typing import Optional
+
+
+def partition_cases(weights, world: int) -> list:
+    """Indices of the cases for each of `world` ranks: largest first, each to
+    the rank with the least work so far (ties to the lower rank), so the
+    ranks' shares of the total work differ by at most the largest case.
+    Deterministic: every rank computes the same partition."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(weights)), key=lambda i: (-weights[i], i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(i)
+        load[r] += weights[i]
+    return [sorted(p) for p in parts]
 
 
 def env() -> tuple:
@@ -58,6 +73,14 @@ class Replicas:
 
     def reduce_sum(self, v: float) -> float:
         return self._reduce(v, None if self._dist is None else self._dist.ReduceOp.SUM)
+
+    def gather(self, obj) -> list:
+        """Every rank's obj (a picklable host value), in rank order."""
+        if self._dist is None:
+            return [obj]
+        out = [None] * self.world
+        self._dist.all_gather_object(out, obj)
+        return out
 
     def whole_job_rate(self, units: float, seconds: float) -> tuple:
         """(units of all ranks / slowest rank's seconds, slowest seconds)."""
