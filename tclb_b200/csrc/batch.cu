@@ -537,6 +537,72 @@ int ensure_graph(tclb_batch* B) {
 
 }  // namespace
 
+namespace {
+
+// Lay out case `slot` in its allocation p, upload its tables and fields,
+// and write its descriptor to the device (the caller registers it).
+int fill_case(tclb_batch* B, int slot, char* p, const CaseLayout& L, const ModelTable* T, int nzones, int nx,
+              int ny, int nz, const uint16_t* flags, const double* settings, const double* zone_settings,
+              int zone_rows, int niter) {
+  BatchCase C;
+  std::memset(&C, 0, sizeof(C));
+  C.buf[0] = p;
+  C.buf[1] = p + L.buf;
+  C.flags = reinterpret_cast<flag_t*>(p + 2 * L.buf);
+  C.zone = p + 2 * L.buf + L.flags;
+  C.glob = reinterpret_cast<double*>(p + 2 * L.buf + L.flags + L.zone);
+  C.stride = L.stride;
+  C.nx = nx;
+  C.ny = ny;
+  C.nz = nz;
+  C.counter = 0;
+  C.remaining = niter;
+  C.active = 1;
+  C.glob_end = (B->paths & TCLB_BATCH_GLOBALS_AT_END) ? 1 : 0;
+  BatchTmaMaps maps;  // host copy of the tensor maps, uploaded below
+  if (L.maps) {
+    const int R = tma_rows_for(B->elem, nx, ny);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; b++)
+      ok = encode_tile_maps(C.buf[b], C.flags, nx, ny, nz, B->I->Q, L.stride, R, &maps.rows[b], &maps.row1[b],
+                            &maps.flags);
+    if (ok) {  // otherwise the case runs the register kernels
+      C.tma_rows = R;
+      C.maps = reinterpret_cast<const BatchTmaMaps*>(p + 2 * L.buf + L.flags + L.zone + L.glob);
+      BCK(cudaMemcpyAsync(const_cast<BatchTmaMaps*>(C.maps), &maps, sizeof(maps), cudaMemcpyHostToDevice,
+                          B->stream));
+    }
+  }
+  for (int i = 0; i < T->nsettings && i < BATCH_MAX_SET; i++) C.s[i] = settings[i];
+  B->I->derive(C);
+  // zonal table: default values, then the caller's rows (zone 0.. zone_rows-1)
+  const int nzs = T->nzonesettings;
+  std::vector<double> zt((size_t)nzones * nzs);
+  for (int z = 0; z < nzones; z++)
+    for (int s = 0; s < nzs; s++) zt[(size_t)z * nzs + s] = T->zone_setting_defaults[s];
+  for (int z = 0; z < zone_rows; z++)
+    for (int s = 0; s < nzs; s++) zt[(size_t)z * nzs + s] = zone_settings[(size_t)z * nzs + s];
+  if (B->precision == TCLB_FP64) {
+    BCK(cudaMemcpyAsync(const_cast<void*>(C.zone), zt.data(), zt.size() * 8, cudaMemcpyHostToDevice, B->stream));
+  } else {
+    std::vector<float> zf(zt.begin(), zt.end());
+    BCK(cudaMemcpyAsync(const_cast<void*>(C.zone), zf.data(), zf.size() * 4, cudaMemcpyHostToDevice, B->stream));
+    BCK(cudaStreamSynchronize(B->stream));
+  }
+  BCK(cudaMemcpyAsync(const_cast<flag_t*>(C.flags), flags, (size_t)nx * ny * nz * sizeof(flag_t),
+                      cudaMemcpyHostToDevice, B->stream));
+  BCK(cudaMemsetAsync(C.glob, 0, B->I->NG * sizeof(double), B->stream));
+  B->I->init(C, C.buf[0], B->stream, 32, 4);
+  BCK(cudaGetLastError());
+  B->cases[slot] = C;
+  int rc = upload_case(B, slot);
+  if (rc) return rc;
+  BCK(cudaStreamSynchronize(B->stream));
+  return TCLB_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* tclb_batch_last_error(void) { return g_batch_err.c_str(); }
@@ -636,64 +702,16 @@ int tclb_batch_add_case(tclb_batch_h B, int nx, int ny, int nz, const uint16_t* 
   }
   char* p = nullptr;
   BCK(cudaMallocFromPoolAsync((void**)&p, L.total, B->pool, B->stream));
-  BatchCase C;
-  std::memset(&C, 0, sizeof(C));
-  C.buf[0] = p;
-  C.buf[1] = p + L.buf;
-  C.flags = reinterpret_cast<flag_t*>(p + 2 * L.buf);
-  C.zone = p + 2 * L.buf + L.flags;
-  C.glob = reinterpret_cast<double*>(p + 2 * L.buf + L.flags + L.zone);
-  C.stride = L.stride;
-  C.nx = nx;
-  C.ny = ny;
-  C.nz = nz;
-  C.counter = 0;
-  C.remaining = niter;
-  C.active = 1;
-  C.glob_end = (B->paths & TCLB_BATCH_GLOBALS_AT_END) ? 1 : 0;
-  BatchTmaMaps maps;  // host copy of the tensor maps, uploaded below
-  if (L.maps) {
-    const int R = tma_rows_for(B->elem, nx, ny);
-    bool ok = true;
-    for (int b = 0; b < 2 && ok; b++)
-      ok = encode_tile_maps(C.buf[b], C.flags, nx, ny, nz, B->I->Q, L.stride, R, &maps.rows[b], &maps.row1[b],
-                            &maps.flags);
-    if (ok) {  // otherwise the case runs the register kernels
-      C.tma_rows = R;
-      C.maps = reinterpret_cast<const BatchTmaMaps*>(p + 2 * L.buf + L.flags + L.zone + L.glob);
-      BCK(cudaMemcpyAsync(const_cast<BatchTmaMaps*>(C.maps), &maps, sizeof(maps), cudaMemcpyHostToDevice,
-                          B->stream));
-    }
+  const int rc = fill_case(B, slot, p, L, T, nzones, nx, ny, nz, flags, settings, zone_settings, zone_rows, niter);
+  if (rc) {  // the allocation goes back to the pool; the slot stays free
+    cudaFreeAsync(p, B->stream);
+    std::memset(&B->cases[slot], 0, sizeof(BatchCase));
+    return rc;
   }
-  for (int i = 0; i < T->nsettings && i < BATCH_MAX_SET; i++) C.s[i] = settings[i];
-  B->I->derive(C);
-  // zonal table: default values, then the caller's rows (zone 0.. zone_rows-1)
-  const int nzs = T->nzonesettings;
-  std::vector<double> zt((size_t)nzones * nzs);
-  for (int z = 0; z < nzones; z++)
-    for (int s = 0; s < nzs; s++) zt[(size_t)z * nzs + s] = T->zone_setting_defaults[s];
-  for (int z = 0; z < zone_rows; z++)
-    for (int s = 0; s < nzs; s++) zt[(size_t)z * nzs + s] = zone_settings[(size_t)z * nzs + s];
-  if (B->precision == TCLB_FP64) {
-    BCK(cudaMemcpyAsync(const_cast<void*>(C.zone), zt.data(), zt.size() * 8, cudaMemcpyHostToDevice, B->stream));
-  } else {
-    std::vector<float> zf(zt.begin(), zt.end());
-    BCK(cudaMemcpyAsync(const_cast<void*>(C.zone), zf.data(), zf.size() * 4, cudaMemcpyHostToDevice, B->stream));
-    BCK(cudaStreamSynchronize(B->stream));
-  }
-  BCK(cudaMemcpyAsync(const_cast<flag_t*>(C.flags), flags, (size_t)nx * ny * nz * sizeof(flag_t),
-                      cudaMemcpyHostToDevice, B->stream));
-  BCK(cudaMemsetAsync(C.glob, 0, B->I->NG * sizeof(double), B->stream));
-  B->I->init(C, C.buf[0], B->stream, 32, 4);
-  BCK(cudaGetLastError());
-  B->cases[slot] = C;
   B->bytes[slot] = L.total;
   B->used_slot[slot] = 1;
   B->used += L.total;
   B->h_status[slot] = make_int2(0, niter);
-  int rc = upload_case(B, slot);
-  if (rc) return rc;
-  BCK(cudaStreamSynchronize(B->stream));
   B->tiles_dirty = true;
   *case_id = slot;
   return TCLB_OK;
