@@ -381,19 +381,43 @@ def porous_box_single(n=128, storage="fp16s", iters=24) -> dict:
     return {"workload": f"single lattice, d3q19 porous box {n}^3, {storage}", "iterations": iters, "path": path}
 
 
+def config4_replays(n_cases=512, storage="same", bx=32, by=32, K=64, replays=2) -> dict:
+    """The config-4 cases in one batch at a fixed launch shape, a few replays
+    (profiling workload: no autotuning, no single-case reference)."""
+    import torch
+
+    specs, _ = batch_specs(n_cases, iterations=1 << 20)
+    b = Batch("d2q9", "fp32", storage=storage, budget_bytes=100 << 30, max_cases=n_cases)
+    b.set_paths(globals_at_end=True)
+    b.set_launch(bx, by, K)
+    for s_ in specs:
+        b.add_case(s_)
+    for _ in range(replays):
+        b.step()
+    b.sync()
+    torch.cuda.synchronize()
+    info = b.info()
+    b.close()
+    return {"workload": f"config-4 batch, {n_cases} d2q9 cases, {storage}, tiles {bx}x{by}, K={K}",
+            "replays": replays, "tiles": info["tiles"], "nodes": sum(int(np.prod(x.shape)) for x in specs)}
+
+
 def main(argv=None):
     import argparse
 
     p = argparse.ArgumentParser(description="profiling workloads (one JSON line)")
-    p.add_argument("what", choices=["porous-box-batch", "porous-box-single"])
+    p.add_argument("what", choices=["porous-box-batch", "porous-box-single", "config4-replays"])
     p.add_argument("--n", type=int, default=128)
+    p.add_argument("--cases", type=int, default=512)
     p.add_argument("--storage", default="fp16s")
     p.add_argument("--no-tma", action="store_true")
     a = p.parse_args(argv)
     if a.what == "porous-box-batch":
         r = porous_box_batch(a.n, a.storage, use_tma=not a.no_tma)
-    else:
+    elif a.what == "porous-box-single":
         r = porous_box_single(a.n, a.storage)
+    else:
+        r = config4_replays(a.cases, a.storage)
     print(json.dumps(r))
 
 
