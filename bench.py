@@ -389,6 +389,7 @@ def run_config(args):
         return 0
     elif args.config == 2:  # --accuracy
         res = BM.config2_accuracy(n=args.n)
+        res["drag"] = BM.sphere_drag_accuracy()
     else:
         res = {1: BM.config1, 3: BM.config3}[args.config]()
     if rank == 0:

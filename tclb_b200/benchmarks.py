@@ -343,6 +343,38 @@ def config2_accuracy(models=("d3q27_cumulant", "d3q19"), n=256, iterations=2000,
     return out
 
 
+def sphere_drag_accuracy(shape=(64, 64, 192), iterations=2000, u_in=0.02, nu=0.02,
+                         storages=("fp32", "fp16s", "bf16s")) -> dict:
+    """d3q27_cumulant flow past a Body-flagged sphere (cases.sphere_channel_d3q27)
+    in each storage next to FP64: relative error of the Drag Global at the
+    last iteration and relative L2 error of the velocity field."""
+    nz, ny, nx = shape
+    fl, zones = cases.sphere_channel_d3q27(nx, ny, nz)
+    res, ref_u, ref_drag = {}, None, None
+    for st in ("fp64",) + tuple(storages):
+        prec = "fp64" if st == "fp64" else "fp32"
+        storage = "same" if st in ("fp64", "fp32") else st
+        lat = Lattice("d3q27_cumulant", nx, ny, nz, precision=prec, storage=storage)
+        lat.set_flags(fl)
+        lat.SetSetting("nu", nu)
+        lat.set_zone_setting("Velocity", u_in, zones["Inlet"])
+        lat.Init()
+        lat.Iterate(iterations, M.ITER_NORM | M.ITER_LASTGLOB)
+        drag = lat.globals_dict()["Drag"]
+        u = lat.GetQuantity("U").astype(np.float64)
+        path = lat.launch_path()
+        lat.close()
+        if st == "fp64":
+            ref_u, ref_drag = u, drag
+            res[st] = {"drag": drag}
+            continue
+        res[st] = {"drag": drag, "drag_rel_err": abs(drag - ref_drag) / abs(ref_drag),
+                   "u_rel_l2_vs_fp64": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u)),
+                   "path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")}
+    return {"config": f"d3q27_cumulant sphere (r = 8) in a {nx}x{ny}x{nz} duct, inlet u = {u_in}, nu = {nu}, "
+                      f"{iterations} iterations", "runs": res}
+
+
 # ---------------------------------------------------------------------------
 # Profiling workloads: one porous d3q19 box (p = 0.08, 2-node wall band, seed
 # 1), n^3 nodes, advanced through a batch (its kernel path chosen by the

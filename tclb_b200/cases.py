@@ -226,6 +226,23 @@ def batch_cases_d2q9(n_cases=512, seed=0, w_min=64, w_max=2048, ux=0.02, re_rang
     return out, clamps
 
 
+def sphere_channel_d3q27(nx=192, ny=64, nz=64, r=8, cx=48) -> Tuple[np.ndarray, Dict[str, int]]:
+    """d3q27_cumulant flow past a sphere in a square duct: velocity inlet
+    (zone Inlet) at x = 0, pressure outlet (zone Outlet) at x = nx-1, walls on
+    the y and z faces, and a sphere of radius r at (cx, ny/2, nz/2) of Wall
+    nodes flagged Body, on which the model accumulates Drag, Lift and Lateral.
+    Returns the node types and the zone indices."""
+    g = Geometry("d3q27_cumulant", nx, ny, nz)
+    g.set_flag("MRT").box()
+    g.set_flag("WVelocity", zone="Inlet").inlet()
+    g.set_flag("EPressure", zone="Outlet").outlet()
+    g.set_flag("Wall", mask="ALL").tunnel()
+    cy, cz = ny // 2, nz // 2
+    g.sphere(dx=cx - r, nx=2 * r, dy=cy - r, ny=2 * r, dz=cz - r, nz=2 * r)
+    g.set_flag("Body").sphere(dx=cx - r, nx=2 * r, dy=cy - r, ny=2 * r, dz=cz - r, nz=2 * r)
+    return g.geom, dict(g.zones)
+
+
 def disc_channel_flags(W, H, r, cx, cy) -> np.ndarray:
     g = Geometry("d2q9", W, H)
     g.set_flag("MRT").box()

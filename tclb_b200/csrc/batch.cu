@@ -105,7 +105,7 @@ template <class M, class R, class St>
 struct BL {
   // launch K-1 of a replay is every case's last iteration: the Globals variant
   static constexpr bool pairs = sizeof(typename St::T) == 2;  // 16-bit storage
-  static size_t tma_smem() { return 128 + (size_t)tma_stages<M>() * (M::Q + 1) * TMA_TILE * 2; }
+  static size_t tma_smem() { return tma_smem_bytes<M>(); }
   static void iterate(const LaunchTables& L, int k, int K, dim3 gp, dim3 ga, int tma_grid, const double* group,
                       int bx, int by, int form, bool plain_last, cudaStream_t s) {
     const dim3 b(bx, block_rows(bx, by, 256));

@@ -106,6 +106,15 @@ constexpr int tma_stages() {
 }
 constexpr int TMA_CONSUMERS = 8;                   // consumer warps per block
 constexpr unsigned TMA_TILE = TMA_CONSUMERS * 64;  // nodes per tile (two per consumer thread)
+
+// Dynamic shared memory of the tile-staged kernels: 128 bytes of mbarriers,
+// then the stages, laid out with the compile-time stride TMA_TILE per
+// population block whatever the tile's R * nx (at most TMA_TILE; 384 when
+// nx = 192), so the allocation must cover the full stride.
+template <class M>
+constexpr size_t tma_smem_bytes() {
+  return 128 + (size_t)tma_stages<M>() * (M::Q + 1) * TMA_TILE * 2;
+}
 constexpr long long TMA_WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
 constexpr int TMA_ERR_TIMEOUT = 1;
 
@@ -251,7 +260,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       }
       if (lane == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * block * 2u);
+        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(R_rows * nx) * 2u);  // the bytes of R_rows rows
       }
       __syncwarp();
       tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);

@@ -219,7 +219,7 @@ struct Launch {
       }
       if (L->use_tma && L->tma_ok && !glob) {  // tiles staged in shared memory by TMA
         const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
-        const size_t smem = 128 + (size_t)tma_stages<M>() * (M::Q + 1) * rows * L->nx * sizeof(T);
+        const size_t smem = tma_smem_bytes<M>();
         if (L->tma_grid > 0) {
           k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev);
           return;
@@ -246,7 +246,7 @@ struct Launch {
     if constexpr (sizeof(T) == 2) {
       if (!L->tma_ok) return;
       const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
-      const size_t smem = 128 + (size_t)tma_stages<M>() * (M::Q + 1) * rows * L->nx * sizeof(T);
+      const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
       if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
               cudaSuccess ||

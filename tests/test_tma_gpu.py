@@ -32,10 +32,12 @@ PARAMS = {
 }
 # (nz, ny, nx): rows per tile = 512 / nx; ny a multiple of it. Small ny makes
 # most tiles wrap at a y face (the one-row copies), larger ny has inner tiles.
+# nx = 192 gives 2-row tiles of 384 nodes: fewer than the 512 of the stage
+# layout, six consumer warps.
 SHAPES = {
-    "d2q9": [(1, 16, 128), (1, 8, 64), (1, 6, 256)],
-    "d3q19": [(4, 8, 64), (3, 12, 128), (3, 6, 256)],
-    "d3q27_cumulant": [(4, 8, 64), (3, 12, 128), (2, 6, 256)],
+    "d2q9": [(1, 16, 128), (1, 8, 64), (1, 6, 256), (1, 8, 192)],
+    "d3q19": [(4, 8, 64), (3, 12, 128), (3, 6, 256), (3, 6, 192)],
+    "d3q27_cumulant": [(4, 8, 64), (3, 12, 128), (2, 6, 256), (2, 8, 192)],
 }
 
 
