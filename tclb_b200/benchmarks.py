@@ -343,14 +343,20 @@ def config2_accuracy(models=("d3q27_cumulant", "d3q19"), n=256, iterations=2000,
     return out
 
 
-def sphere_drag_accuracy(shape=(64, 64, 192), iterations=2000, u_in=0.02, nu=0.02,
+def sphere_drag_accuracy(shape=(128, 128, 256), r=12, cx=64, iterations=2000, u_in=0.02, nu=0.02,
                          storages=("fp32", "fp16s", "bf16s")) -> dict:
     """d3q27_cumulant flow past a Body-flagged sphere (cases.sphere_channel_d3q27)
     in each storage next to FP64: relative error of the Drag Global at the
-    last iteration and relative L2 error of the velocity field."""
+    last iteration, relative L2 error of the velocity field, and the rate
+    (MLUPS, CUDA events around the whole run of plain iterations and the
+    final Globals one) with the kernel path taken."""
+    import torch
+
     nz, ny, nx = shape
-    fl, zones = cases.sphere_channel_d3q27(nx, ny, nz)
+    fl, zones = cases.sphere_channel_d3q27(nx, ny, nz, r=r, cx=cx)
     res, ref_u, ref_drag = {}, None, None
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
     for st in ("fp64",) + tuple(storages):
         prec = "fp64" if st == "fp64" else "fp32"
         storage = "same" if st in ("fp64", "fp32") else st
@@ -359,20 +365,33 @@ def sphere_drag_accuracy(shape=(64, 64, 192), iterations=2000, u_in=0.02, nu=0.0
         lat.SetSetting("nu", nu)
         lat.set_zone_setting("Velocity", u_in, zones["Inlet"])
         lat.Init()
-        lat.Iterate(iterations, M.ITER_NORM | M.ITER_LASTGLOB)
+        lat.Iterate(8, stream=sp)  # graph capture, warm-up
+        lat.Init()
+        a, b = _events(torch, stream)
+        torch.cuda.synchronize()
+        a.record(stream)
+        lat.Iterate(iterations - 1, M.ITER_NORM, stream=sp)
+        lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        b.record(stream)
+        torch.cuda.synchronize()
+        mlups = lat.N * iterations / (a.elapsed_time(b) / 1e3) / 1e6
         drag = lat.globals_dict()["Drag"]
         u = lat.GetQuantity("U").astype(np.float64)
         path = lat.launch_path()
         lat.close()
         if st == "fp64":
             ref_u, ref_drag = u, drag
-            res[st] = {"drag": drag}
+            res[st] = {"drag": drag, "MLUPS": mlups}
             continue
         res[st] = {"drag": drag, "drag_rel_err": abs(drag - ref_drag) / abs(ref_drag),
-                   "u_rel_l2_vs_fp64": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u)),
+                   "u_rel_l2_vs_fp64": float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u)), "MLUPS": mlups,
                    "path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one")}
-    return {"config": f"d3q27_cumulant sphere (r = 8) in a {nx}x{ny}x{nz} duct, inlet u = {u_in}, nu = {nu}, "
-                      f"{iterations} iterations", "runs": res}
+    if "fp32" in res:
+        for st in storages:
+            if st != "fp32":
+                res[st]["speedup_vs_fp32"] = res[st]["MLUPS"] / res["fp32"]["MLUPS"]
+    return {"config": f"d3q27_cumulant sphere (r = {r}, Body-flagged walls) in a {nx}x{ny}x{nz} duct, inlet "
+                      f"u = {u_in}, nu = {nu}, {iterations} iterations", "runs": res}
 
 
 # ---------------------------------------------------------------------------
