@@ -131,11 +131,12 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-def profiled_traffic(model, precision, storage, n):
+def profiled_traffic(kernel, model, precision, storage, n):
     """DRAM bytes per launch of the iteration kernel from the committed ncu
-    summary of this workload, if one exists (line 'traffic_bytes_per_launch: X'
-    under a heading naming the workload)."""
-    path = os.path.join(ROOT, "profiles", f"k_iterate_{model}_{precision}_{storage}_{n}.md")
+    summary of this kernel and workload, if one exists
+    (profiles/<kernel>_<model>_<precision>_<storage>_<n>.md, line
+    'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{model}_{precision}_{storage}_{n}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -319,10 +320,11 @@ def run_ours(args):
 
     peaks, peak_src = measured_peaks()
     achieved = bpu * N / kern / 1e9
-    traffic = profiled_traffic(args.model, args.precision, args.storage, n)
+    kernel = "k_iterate_tma" if path["tma"] else ("k_iterate_pair" if path["pairs"] else "k_iterate")
+    traffic = profiled_traffic(kernel, args.model, args.precision, args.storage, n)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
-            "kernel": "k_iterate (no-Globals variant)", "bytes_per_update": bpu,
+            "kernel": kernel + (" (no-Globals variant)" if kernel == "k_iterate" else ""), "bytes_per_update": bpu,
             "kernel_ms": kern * 1e3, "kernel_mlups": N / kern / 1e6}
 
     # ---- end to end through the C ABI from pinned host buffers -------------
