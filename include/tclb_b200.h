@@ -221,7 +221,8 @@ typedef struct tclb_batch* tclb_batch_h;
 const char* tclb_batch_last_error(void);
 
 /* Device bytes one case occupies (two snapshots, node types, zonal table,
-   Globals): the footprint admission is judged on. */
+   Globals, and tensor maps where the tile-staged kernel applies): the
+   footprint that admission compares with the budget. */
 size_t tclb_batch_case_bytes(int model, int precision, int storage, int nx, int ny, int nz);
 
 /* A batch admits cases while the sum of their footprints stays within

@@ -501,8 +501,8 @@ struct Lattice {
   std::vector<double> zone;  // zones * nzs
   int nzones;
   // Globals are kept as 2*nglob values: the sums, then the sums of absolute
-  // contributions (the scale against which summation and rounding differences
-  // are judged by the tests).
+  // contributions (the scale the tests measure summation and rounding
+  // differences against).
   std::vector<double> dev_globals;  // per-iteration integrated globals (device side in TCLB)
   std::vector<double> globals;      // host accumulators (Lattice::globals)
   long iter = 0;
