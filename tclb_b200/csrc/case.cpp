@@ -9,6 +9,8 @@
 // Solver::outIterFile (src/Solver.h.Rt:102-105).
 #include <sys/stat.h>
 
+#include <array>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -34,55 +36,246 @@ struct CaseError : std::runtime_error {
 };
 
 // ------------------------------------------------------------------ units
-// Values are numbers with an optional unit expression ("0.01", "1m/s",
-// "5mm", "1e-3m2/s"); sums of terms ("1m+2mm") are added (UnitEnv::alt,
-// src/unit.h:160-194). Without <Units> gauges every base unit has scale 1, so
-// a value is its number times the factors of prefixed units.
-double unit_factor(const std::string& u) {
-  static const std::map<std::string, double> pref = {
-      {"nm", 1e-9}, {"um", 1e-6}, {"mm", 1e-3}, {"cm", 1e-2}, {"km", 1e3}, {"h", 3600}, {"ns", 1e-9},
-      {"us", 1e-6}, {"ms", 1e-3}, {"N", 1}, {"Pa", 1}, {"J", 1}, {"W", 1}, {"V", 1}, {"C", 1}};
-  double f = 1.0;
-  size_t i = 0;
-  int sign = 1;
-  while (i < u.size()) {
-    if (u[i] == '/') { sign = -1; i++; continue; }
-    size_t j = i;
-    while (j < u.size() && isalpha((unsigned char)u[j])) j++;
-    size_t k = j;
-    while (k < u.size() && (isdigit((unsigned char)u[k]) || u[k] == '.')) k++;
-    const std::string sym = u.substr(i, j - i);
-    const double p = k > j ? std::atof(u.substr(j, k - j).c_str()) : 1.0;
-    // longest known prefixed unit first, else base units (scale 1)
-    size_t q = 0;
-    double ff = 1.0;
-    while (q < sym.size()) {
-      if (q + 2 <= sym.size() && pref.count(sym.substr(q, 2))) { ff *= pref.at(sym.substr(q, 2)); q += 2; }
-      else if (pref.count(sym.substr(q, 1))) { ff *= pref.at(sym.substr(q, 1)); q += 1; }
-      else q += 1;
-    }
-    f *= std::pow(ff, sign * p);
-    if (k == i) k++;
-    i = k;
-  }
-  return f;
+// TCLB's unit system (src/unit.h, src/unit.cpp): a quantity is a number
+// times powers of nine base units (m, s, kg, K, x, y, z, A, t). A value is a
+// sum of terms ("1m+2mm"), each a number and unit tokens: letters then an
+// optional power ("m2"), and one "/" after which every token divides
+// ("1kgm/s2"). A letter group splits into known one- or two-letter symbols;
+// where both splits are valid a leading "m" is read as milli, any other
+// ambiguity is an error. <Units> gauges (<Param value="1m" gauge="100"/>:
+// that much is one lattice unit's worth of it, here 100) fix a scale per base
+// unit: the gauged quantities must come out as 1 in lattice units, which is a
+// linear system in the logarithms of the scales; base units that no gauge
+// involves keep scale 1, and the system must be square. A value's lattice
+// number is its number times the scales to the powers of its units.
+// Difference: an unknown unit symbol is an error here (TCLB reads it as 0).
+constexpr int NBASE = 9;
+const char* const BASE_UNITS[NBASE] = {"m", "s", "kg", "K", "x", "y", "z", "A", "t"};
+
+struct UVal {
+  double v = 1.0;
+  double e[NBASE] = {};
+  bool valid() const { return v != 0.0; }
+};
+UVal umul(const UVal& a, const UVal& b) {
+  UVal r;
+  r.v = a.v * b.v;
+  for (int i = 0; i < NBASE; i++) r.e[i] = a.e[i] + b.e[i];
+  return r;
+}
+UVal udiv(const UVal& a, const UVal& b) {
+  UVal r;
+  r.v = a.v / b.v;
+  for (int i = 0; i < NBASE; i++) r.e[i] = a.e[i] - b.e[i];
+  return r;
+}
+UVal upow(const UVal& a, double p) {
+  UVal r;
+  r.v = std::pow(a.v, p);
+  for (int i = 0; i < NBASE; i++) r.e[i] = a.e[i] * p;
+  return r;
 }
 
-double parse_value(const std::string& s) {
-  double ret = 0;
-  size_t i = 0;
-  while (i < s.size()) {
-    size_t j = i + 1;
-    while (j < s.size() && !((s[j] == '+' || s[j] == '-') && !(s[j - 1] == 'e' || s[j - 1] == 'E'))) j++;
-    const std::string term = s.substr(i, j - i);
-    char* end = nullptr;
-    const double v = std::strtod(term.c_str(), &end);
-    if (end == term.c_str()) throw CaseError("cannot read value '" + s + "'");
-    ret += v * unit_factor(std::string(end));
-    i = j;
+class UnitEnv {
+ public:
+  UnitEnv() {
+    for (int i = 0; i < NBASE; i++) {
+      UVal b;
+      b.e[i] = 1;
+      units_[BASE_UNITS[i]] = b;
+      scale_[i] = 1.0;
+    }
+    const std::pair<const char*, const char*> derived[] = {
+        {"N", "1kgm/s2"}, {"Pa", "1N/m2"}, {"J", "1Nm"},     {"W", "1J/s"},     {"V", "1kgm2/t3/A"},
+        {"C", "1tA"},     {"nm", "1e-9m"}, {"um", "1e-6m"},  {"mm", "1e-3m"},   {"cm", "1e-2m"},
+        {"km", "1e+3m"},  {"h", "3600s"},  {"ns", "1e-9s"},  {"us", "1e-6s"},   {"ms", "1e-3s"},
+        {"g", "1e-3kg"},  {"mg", "1e-6kg"}};
+    for (const auto& d : derived) units_[d.first] = text(d.second);  // in order: later ones use earlier
+    UVal c;
+    c.v = std::acos(-1.0) / 180.0;
+    units_["d"] = c;  // degree
+    c.v = 0.01;
+    units_["%"] = c;
+    c.v = 6.022e23;
+    units_["An"] = c;
   }
-  return ret;
+
+  UVal text(const std::string& s) const {  // a number, then units
+    char* end = nullptr;
+    double v = std::strtod(s.c_str(), &end);
+    if (end == s.c_str()) {  // units alone ("s"): one of them
+      if (s.empty() || !std::isalpha((unsigned char)s[0])) throw CaseError("cannot read value '" + s + "'");
+      v = 1.0;
+    }
+    UVal r = unit(std::string(end), s);
+    r.v *= v;
+    return r;
+  }
+
+  // lattice value of a value text (sum of terms)
+  double alt(const std::string& s) const {
+    double ret = 0;
+    size_t i = 0;
+    while (i < s.size()) {
+      size_t j = i + 1;
+      while (j < s.size() && !((s[j] == '+' || s[j] == '-') && !(s[j - 1] == 'e' || s[j - 1] == 'E'))) j++;
+      ret += alt(text(s.substr(i, j - i)));
+      i = j;
+    }
+    return ret;
+  }
+  double alt(const UVal& u) const {
+    double r = u.v;
+    for (int i = 0; i < NBASE; i++)
+      if (u.e[i] != 0) r *= std::pow(scale_[i], u.e[i]);
+    return r;
+  }
+
+  void set_gauge(const std::string& name, const std::string& value, const std::string& gauge) {
+    gauges_[name] = udiv(text(value), text(gauge));
+  }
+
+  // the scales: every gauged quantity equals 1 in lattice units
+  void make_gauge() {
+    std::vector<std::array<double, NBASE + 1>> rows;  // coefficients of log(1/scale), right-hand side
+    for (const auto& g : gauges_) {
+      std::array<double, NBASE + 1> r{};
+      for (int j = 0; j < NBASE; j++) r[j] = g.second.e[j];
+      r[NBASE] = std::log(g.second.v);
+      rows.push_back(r);
+    }
+    for (int j = 0; j < NBASE; j++) {  // base units no gauge involves keep scale 1
+      bool used = false;
+      for (const auto& g : gauges_) used |= g.second.e[j] != 0;
+      if (!used) {
+        std::array<double, NBASE + 1> r{};
+        r[j] = 1;
+        rows.push_back(r);
+      }
+    }
+    if (rows.size() > (size_t)NBASE) throw CaseError("<Units>: gauges over-determine the units");
+    if (rows.size() < (size_t)NBASE) throw CaseError("<Units>: gauges under-determine the units");
+    // Gaussian elimination with partial pivoting
+    for (int c = 0; c < NBASE; c++) {
+      int p = c;
+      for (int r = c + 1; r < NBASE; r++)
+        if (std::fabs(rows[r][c]) > std::fabs(rows[p][c])) p = r;
+      if (std::fabs(rows[p][c]) < 1e-12) throw CaseError("<Units>: gauges are not independent");
+      std::swap(rows[c], rows[p]);
+      for (int r = 0; r < NBASE; r++) {
+        if (r == c || rows[r][c] == 0) continue;
+        const double f = rows[r][c] / rows[c][c];
+        for (int k = c; k <= NBASE; k++) rows[r][k] -= f * rows[c][k];
+      }
+    }
+    for (int j = 0; j < NBASE; j++) scale_[j] = std::exp(-rows[j][NBASE] / rows[j][j]);
+  }
+  double scale(int j) const { return scale_[j]; }
+
+ private:
+  UVal one(const std::string& sym) const {
+    auto it = units_.find(sym);
+    if (it == units_.end()) {
+      UVal z;
+      z.v = 0;
+      return z;
+    }
+    return it->second;
+  }
+  // a letter group with power p on its last symbol
+  UVal alpha(const std::string& s, double p, const std::string& whole) const {
+    UVal r1 = one(s.substr(0, 1));
+    if (s.size() < 2) return upow(r1, p);
+    r1 = umul(r1, alpha(s.substr(1), p, whole));
+    UVal r2 = one(s.substr(0, 2));
+    r2 = s.size() > 2 ? umul(r2, alpha(s.substr(2), p, whole)) : upow(r2, p);
+    if (!r1.valid()) return r2;
+    if (!r2.valid()) return r1;
+    if (s[0] == 'm') return r2;  // "ms", "mm", "mg": the milli reading
+    throw CaseError("ambiguous unit '" + s + "' in '" + whole + "'");
+  }
+  UVal unit(const std::string& u, const std::string& whole) const {
+    UVal ret;
+    int w = 1;
+    size_t i = 0;
+    while (i < u.size()) {
+      const size_t j = i;
+      while (i < u.size() && std::isalpha((unsigned char)u[i])) i++;
+      const size_t k = i;
+      while (i < u.size() && (std::isdigit((unsigned char)u[i]) || u[i] == '.')) i++;
+      const double p = i > k ? std::atof(u.substr(k, i - k).c_str()) : 1.0;
+      if (k > j) {
+        const UVal last = alpha(u.substr(j, k - j), p, whole);
+        if (!last.valid()) throw CaseError("unknown unit '" + u.substr(j, k - j) + "' in '" + whole + "'");
+        ret = w > 0 ? umul(ret, last) : udiv(ret, last);
+      }
+      const size_t q = i;
+      while (i < u.size() && !std::isalnum((unsigned char)u[i])) i++;
+      if (i - q > 1) throw CaseError("more than one separator in the units of '" + whole + "'");
+      if (i - q == 1) {
+        if (u[q] != '/') throw CaseError("only '/' may separate units in '" + whole + "'");
+        w = -1;
+      }
+    }
+    return ret;
+  }
+
+  std::map<std::string, UVal> units_;
+  std::map<std::string, UVal> gauges_;  // by name, as given in <Units>
+  double scale_[NBASE];
+};
+
+// The unit environment of the case being read (gauged by its <Units>).
+thread_local UnitEnv g_units;
+
+// <Units>: reset the environment and gauge it (before anything else is read,
+// as src/main.cpp:31-62 does).
+void read_units(const XmlNode* cfg) {
+  g_units = UnitEnv();
+  const XmlNode* u = cfg ? cfg->child("Units") : nullptr;
+  if (u) {
+    int k = 1;
+    for (const auto& c : u->children) {
+      if (c->name != "Param") continue;
+      const std::string* v = c->attr("value");
+      const std::string* g = c->attr("gauge");
+      if (!v) throw CaseError("<Units><Param> without a value");
+      if (!g) throw CaseError("<Units><Param> without a gauge");
+      g_units.set_gauge(c->attr_or("name", "unnamed" + std::to_string(k)), *v, *g);
+      k++;
+    }
+  }
+  g_units.make_gauge();
 }
+
+double parse_value(const std::string& s) { return g_units.alt(s); }
+
+// Units of the settings, zonal settings and Globals that have one (unit= of
+// AddSetting / AddGlobal in models/flow/<model>/Dynamics.R); all others are
+// dimensionless ("1").
+const char* quantity_unit(int model, const std::string& name) {
+  static const std::map<std::string, const char*> d2q9 = {
+      {"PressureLoss", "1mPa"}, {"OutletFlux", "1m2/s"}, {"InletFlux", "1m2/s"}};
+  static const std::map<std::string, const char*> d3q19 = {
+      {"nu", "1m2/s"},    {"InletVelocity", "1m/s"}, {"InletPressure", "1Pa"}, {"InletDensity", "1kg/m3"},
+      {"Flux", "m3/s"},   {"XYvx", "m3/s"},          {"XYvy", "m3/s"},         {"XYvz", "m3/s"},
+      {"XYrho", "kg/m"},  {"XYarea", "m2"},          {"XZvx", "m3/s"},         {"XZvy", "m3/s"},
+      {"XZvz", "m3/s"},   {"XZrho", "kg/m"},         {"XZarea", "m2"},         {"YZvx", "m3/s"},
+      {"YZvy", "m3/s"},   {"YZvz", "m3/s"},          {"YZrho", "kg/m"},        {"YZarea", "m2"},
+      {"VOLvx", "m4/s"},  {"VOLvy", "m4/s"},         {"VOLvz", "m4/s"},        {"VOLpx", "mkg/s"},
+      {"VOLpy", "mkg/s"}, {"VOLpz", "mkg/s"},        {"VOLrho", "kg"},         {"VOLvolume", "m3"},
+      {"MaxV", "m3"}};
+  static const std::map<std::string, const char*> d3q27c = {
+      {"Density", "kg/m3"}, {"Flux", "m3/s"}, {"Drag", "N"},         {"Lift", "N"},         {"Lateral", "N"},
+      {"Mass", "kg"},       {"XMomentum", "kgm/s"}, {"YMomentum", "kgm/s"}, {"ZMomentum", "kgm/s"}};
+  const std::map<std::string, const char*>& m = model == MODEL_D2Q9 ? d2q9 : (model == MODEL_D3Q19 ? d3q19 : d3q27c);
+  const auto it = m.find(name);
+  return it == m.end() ? "1" : it->second;
+}
+
+// Multiplier from a lattice value to SI for the Log's _si columns
+// (LogScales, src/Solver.cpp.Rt:145-159): 1 / (lattice value of one unit).
+double si_scale(int model, const std::string& name) { return 1.0 / g_units.alt(quantity_unit(model, name)); }
 
 int parse_int(const std::string& s) { return (int)std::lround(parse_value(s)); }
 
@@ -423,7 +616,9 @@ struct Runner {
     return outpath + "_" + name + buf + suffix;
   }
 
-  // Solver::initLog / writeLog (src/Solver.cpp.Rt:120-206); no <Units>: every scale is 1
+  // Solver::initLog / writeLog (src/Solver.cpp.Rt:120-206): each value and its
+  // SI value (si_scale), then the SI sizes of the lattice units of length,
+  // time and mass; Time_si is the iteration times that of time.
   void log_header(const std::string& f) {
     FILE* o = std::fopen(f.c_str(), "wt");
     if (!o) throw CaseError("cannot write " + f);
@@ -442,22 +637,24 @@ struct Runner {
     FILE* o = std::fopen(f.c_str(), "at");
     if (!o) throw CaseError("cannot write " + f);
     const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    std::fprintf(o, "%lld, %.13le, %.13le, %d", iter, (double)iter, wall, 0);
+    const double dt_si = 1.0 / g_units.alt("s");
+    std::fprintf(o, "%lld, %.13le, %.13le, %d", iter, dt_si * (double)iter, wall, 0);
     for (int i = 0; i < T->nsettings; i++) {
       double v = 0;
       tclb_get_setting(lat, i, &v);
-      std::fprintf(o, ", %.13le, %.13le", v, v);
+      std::fprintf(o, ", %.13le, %.13le", v, v * si_scale(model, T->setting_names[i]));
     }
     for (int i = 0; i < T->nzonesettings; i++)
       for (const auto& z : geo->zones) {
         double v = 0;
         tclb_get_zone_setting(lat, i, z.second, &v);
-        std::fprintf(o, ", %.13le, %.13le", v, v);
+        std::fprintf(o, ", %.13le, %.13le", v, v * si_scale(model, T->zone_setting_names[i]));
       }
     std::vector<double> g(T->nglobals);
     tclb_get_globals(lat, g.data());
-    for (double v : g) std::fprintf(o, ", %.13le, %.13le", v, v);
-    for (int i = 0; i < 3; i++) std::fprintf(o, ", %.13le", 1.0);
+    for (int i = 0; i < T->nglobals; i++)
+      std::fprintf(o, ", %.13le, %.13le", g[i], g[i] * si_scale(model, T->global_names[i]));
+    for (const char* u : {"m", "s", "kg"}) std::fprintf(o, ", %.13le", 1.0 / g_units.alt(u));
     std::fprintf(o, "\n");
     std::fclose(o);
   }
@@ -668,8 +865,7 @@ struct Runner {
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint")
         callback(n);
       else if (n->name == "LoadBinary") load_binary(n);
-      else if (n->name == "Units") {
-        if (!n->children.empty()) throw CaseError("<Units> gauges are not supported: give values in lattice units");
+      else if (n->name == "Units") {  // read before the run (read_units)
       } else if (n->name == "VTK" || n->name == "TXT" || n->name == "Stop" || n->name == "Average") {
         if (verbose) std::printf("[tclb_run] <%s> is not supported; skipped\n", n->name.c_str());
       } else {
@@ -735,6 +931,7 @@ int tclb_case_geometry(const char* xml_text, int model, int dims[3], uint16_t* f
     if (!T) throw CaseError("unknown model");
     auto doc = XmlParser(xml_text).parse();
     const XmlNode* cfg = doc->child("CLBConfig");
+    read_units(cfg);
     const XmlNode* g = cfg ? cfg->child("Geometry") : doc->child("Geometry");
     if (!g) throw CaseError("no <Geometry> element");
     const int nx = pad_nx(parse_int(g->attr_or("nx", "1"))), ny = parse_int(g->attr_or("ny", "1")),
@@ -770,6 +967,7 @@ int tclb_case_run(const char* xml_path, int model, int precision, int storage, c
     auto doc = XmlParser(text).parse();
     const XmlNode* cfg = doc->child("CLBConfig");
     if (!cfg) throw CaseError("no <CLBConfig> element");
+    read_units(cfg);
     std::string base = xml_path;
     const size_t sl = base.find_last_of('/');
     if (sl != std::string::npos) base = base.substr(sl + 1);

@@ -99,6 +99,64 @@ def test_bad_case_is_an_error_not_an_exit():
     assert rc != 0 and b"XML" in lib.tclb_case_last_error()
 
 
+def test_units_gauges_scale_the_geometry():
+    """<Units> gauges (1 mm = 1 lattice length, 1e-6 m2/s = 0.02) make the
+    SI version of the channel case rasterise exactly like the lattice one."""
+    plain = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    si = open(os.path.join(HERE, "cases", "channel_disc_si.xml")).read()
+    a, b = case_geometry(plain, "d2q9"), case_geometry(si, "d2q9")
+    assert a.shape == b.shape and np.array_equal(a, b)
+
+
+def test_units_errors():
+    """Gauges that fix one base unit twice, and unknown unit symbols, are errors
+    (status codes with a message), not silent zeros."""
+    lib = load_library()
+    dims = (ctypes.c_int * 3)()
+    over = (b"<CLBConfig><Units><Param value='1m' gauge='10'/><Param value='2m' gauge='5'/></Units>"
+            b"<Geometry nx='8' ny='8'/></CLBConfig>")
+    assert lib.tclb_case_geometry(over, 0, dims, None, 0) != 0
+    assert b"over-determine" in lib.tclb_case_last_error()
+    unknown = b"<CLBConfig><Geometry nx='8qq' ny='8'/></CLBConfig>"
+    assert lib.tclb_case_geometry(unknown, 0, dims, None, 0) != 0
+    assert b"unknown unit" in lib.tclb_case_last_error()
+    ok = b"<CLBConfig><Units><Param value='1cm' gauge='4'/></Units><Geometry nx='8cm' ny='2cm+1mm'/></CLBConfig>"
+    assert lib.tclb_case_geometry(ok, 0, dims, None, 0) == 0
+    assert list(dims) == [32, 8, 1]  # nx 32 (already a multiple of 32), ny round(8.4)
+
+
+@pytest.mark.gpu
+def test_case_file_run_with_units(tmp_path):
+    """The SI version of the channel case through tclb_run: the same lattice
+    values as the plain case (Log value columns), SI columns scaled by the
+    gauges (1 s = 50 iterations, 1 mm = 1), Time_si the iteration in seconds."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    res = {}
+    for name in ("channel_disc", "channel_disc_si"):
+        out = str(tmp_path / name) + "/"
+        r = subprocess.run([runner, "d2q9", os.path.join(HERE, "cases", name + ".xml"), "--output", out, "--quiet"],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        rows = open(glob.glob(out + name + "_Log_P00_00000000.csv")[0]).read().strip().splitlines()
+        hdr = [h.strip('"') for h in rows[0].split(",")]
+        res[name] = (hdr, np.array([[float(v) for v in row.split(",")] for row in rows[1:]]))
+    (hp, dp), (hs, ds) = res["channel_disc"], res["channel_disc_si"]
+    assert hp == hs and list(ds[:, 0]) == [50, 100, 150, 200]
+    for col in ("Viscosity", "VelocityX-Inlet", "PressureLoss", "OutletFlux", "InletFlux"):
+        i = hp.index(col)
+        assert ds[:, i] == pytest.approx(dp[:, i], rel=1e-5, abs=1e-12), col
+    assert ds[:, hs.index("Time_si")] == pytest.approx(ds[:, 0] / 50)
+    assert ds[-1, hs.index("dx_si")] == pytest.approx(1e-3) and ds[-1, hs.index("dt_si")] == pytest.approx(0.02)
+    assert ds[-1, hs.index("dm_si")] == pytest.approx(1.0)
+    # PressureLoss is in mPa = kg/s2: one lattice unit of it is 1 / 50^2 of one, so SI = lattice * 2500
+    i = hs.index("PressureLoss")
+    assert ds[:, i + 1] == pytest.approx(ds[:, i] * 2500, rel=1e-9)
+    # the plain case has no gauges: SI columns equal the lattice ones
+    assert dp[:, i + 1] == pytest.approx(dp[:, i], rel=1e-12)
+
+
 @pytest.mark.gpu
 def test_case_file_run_matches_api(tmp_path):
     """tclb_run on the channel case: the Log CSV rows and the final BIN files
