@@ -515,11 +515,21 @@ struct Runner;
 std::string read_file(const std::string& path);
 void write_xml(std::ostream& o, const XmlNode* n, int depth);
 
+// The previous value of a <Stop> criterion before its first check (cbStop's
+// own sentinel, so a first Change check fails as in TCLB).
+constexpr double STOP_UNSET = -12341234;
+
 struct Callback {
-  std::string kind;  // Log, BIN, Failcheck
+  std::string kind;  // Log, BIN, Failcheck, SaveCheckpoint, Stop
   const XmlNode* node;
   double every = 0, start = 0;
   std::string file;
+  // <Stop> (src/Handlers/cbStop.cpp): per criterion the Global, its kind,
+  // limit and value at the previous check; consecutive passing checks
+  enum { CHANGE, PERCENT_CHANGE, ABOVE, BELOW };
+  std::vector<int> stop_global, stop_kind;
+  std::vector<double> stop_limit, stop_old;
+  int stop_times = 1, stop_score = 0;
   bool now(double it) const {  // vHandler::Now
     if (every <= 0) return false;
     it -= start;
@@ -796,6 +806,26 @@ struct Runner {
       log_header(c.file);
       iter_type |= TCLB_ITER_LASTGLOB;  // cbLog::Init
     }
+    if (c.kind == "Stop") {  // cbStop::Init
+      const char* suffix[4] = {"Change", "PercentChange", "Above", "Below"};
+      for (int g = 0; g < T->nglobals; g++)
+        for (int k = 0; k < 4; k++)
+          if (const std::string* v = n->attr(std::string(T->global_names[g]) + suffix[k])) {
+            char* end = nullptr;
+            const double lim = std::strtod(v->c_str(), &end);
+            if (end == v->c_str()) throw CaseError("<Stop>: cannot read " + *v);
+            c.stop_global.push_back(g);
+            c.stop_kind.push_back(k);
+            c.stop_limit.push_back(lim);
+            c.stop_old.push_back(STOP_UNSET);
+          }
+      if (c.stop_global.empty()) throw CaseError("<Stop> names no <Global>Change/PercentChange/Above/Below");
+      if (const std::string* t = n->attr("Times")) {
+        c.stop_times = std::atoi(t->c_str());
+        if (c.stop_times < 1) throw CaseError("<Stop> Times must be at least 1");
+      }
+      iter_type |= TCLB_ITER_LASTGLOB;  // the Globals it checks
+    }
     if (c.every > 0) {
       hands.push_back(c);
       return true;
@@ -803,8 +833,32 @@ struct Runner {
     do_callback(c);  // no Iterations: runs once, now (GenericAction::ExecuteInternal)
     return false;
   }
+  // cbStop::DoIt: true when every criterion has held on Times consecutive checks
+  bool stop_check(Callback& c) {
+    std::vector<double> g(T->nglobals);
+    tclb_get_globals(lat, g.data());
+    bool miss = false;
+    for (size_t i = 0; i < c.stop_global.size(); i++) {
+      const double v = g[c.stop_global[i]], old = c.stop_old[i], lim = c.stop_limit[i];
+      switch (c.stop_kind[i]) {
+        case Callback::CHANGE: miss |= std::fabs(old - v) > lim; break;
+        case Callback::PERCENT_CHANGE: miss |= std::fabs((old - v) / v) > lim; break;
+        case Callback::ABOVE: miss |= v < lim; break;
+        case Callback::BELOW: miss |= v > lim; break;
+      }
+      c.stop_old[i] = v;
+    }
+    c.stop_score = miss ? 0 : c.stop_score + 1;
+    if (c.stop_score < c.stop_times) return false;
+    std::fill(c.stop_old.begin(), c.stop_old.end(), STOP_UNSET);
+    c.stop_score = 0;
+    if (verbose) std::printf("[tclb_run] Stop at iteration %lld\n", iter);
+    return true;
+  }
+
   // returns true to stop the solve
-  bool do_callback(const Callback& c) {
+  bool do_callback(Callback& c) {
+    if (c.kind == "Stop") return stop_check(c);
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
@@ -840,7 +894,7 @@ struct Runner {
       if (next == my_next) type |= TCLB_ITER_LASTGLOB;
       ck(tclb_iterate(lat, next, type, nullptr), "iterate");
       iter += next;
-      for (const auto& h : hands)
+      for (auto& h : hands)
         if (h.now((double)iter) && do_callback(h)) stop = true;
       if (stop) break;
     } while (!self.now((double)iter));
@@ -862,11 +916,12 @@ struct Runner {
       } else if (n->name == "Param") param(n);
       else if (n->name == "Init") init();
       else if (n->name == "Solve") solve(n);
-      else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint")
+      else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
+               n->name == "Stop")
         callback(n);
       else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)
-      } else if (n->name == "VTK" || n->name == "TXT" || n->name == "Stop" || n->name == "Average") {
+      } else if (n->name == "VTK" || n->name == "TXT" || n->name == "Average") {
         if (verbose) std::printf("[tclb_run] <%s> is not supported; skipped\n", n->name.c_str());
       } else {
         throw CaseError("unsupported element <" + n->name + ">");

@@ -158,6 +158,35 @@ def test_case_file_run_with_units(tmp_path):
 
 
 @pytest.mark.gpu
+def test_stop_ends_the_solve(tmp_path):
+    """<Stop> (cbStop): every criterion holding on Times consecutive checks
+    ends the enclosing <Solve>; a Change criterion's first check never holds;
+    a Stop without criteria is an error."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    plain = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    head = plain[:plain.index("<Log")]
+
+    def run(solve):
+        path = tmp_path / "case.xml"
+        path.write_text(head + '<Log Iterations="50"/>' + solve + "</CLBConfig>")
+        out = str(tmp_path / "out") + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        if r.returncode != 0:
+            return None, r.stderr + r.stdout
+        rows = open(out + "case_Log_P00_00000000.csv").read().strip().splitlines()[1:]
+        return [int(row.split(",")[0]) for row in rows], ""
+
+    its, err = run('<Solve Iterations="100000"><Stop InletFluxAbove="-1e30" Times="2" Iterations="50"/></Solve>')
+    assert its == [50, 100], err
+    its, err = run('<Solve Iterations="300"><Stop PressureLossChange="0" Iterations="50"/></Solve>')
+    assert its == [50, 100, 150, 200, 250, 300], err
+    its, err = run('<Solve Iterations="300"><Stop Times="2" Iterations="50"/></Solve>')
+    assert its is None and "Stop" in err
+
+
+@pytest.mark.gpu
 def test_case_file_run_matches_api(tmp_path):
     """tclb_run on the channel case: the Log CSV rows and the final BIN files
     equal what the Python API produces for the same flags and settings."""
