@@ -9,6 +9,7 @@
 // Solver::outIterFile (src/Solver.h.Rt:102-105).
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <array>
 #include <cctype>
 #include <chrono>
@@ -250,12 +251,12 @@ void read_units(const XmlNode* cfg) {
 
 double parse_value(const std::string& s) { return g_units.alt(s); }
 
-// Units of the settings, zonal settings and Globals that have one (unit= of
-// AddSetting / AddGlobal in models/flow/<model>/Dynamics.R); all others are
-// dimensionless ("1").
+// Units of the settings, zonal settings, Globals and quantities that have one
+// (unit= of AddSetting / AddGlobal / AddQuantity in
+// models/flow/<model>/Dynamics.R); all others are dimensionless ("1").
 const char* quantity_unit(int model, const std::string& name) {
   static const std::map<std::string, const char*> d2q9 = {
-      {"PressureLoss", "1mPa"}, {"OutletFlux", "1m2/s"}, {"InletFlux", "1m2/s"}};
+      {"PressureLoss", "1mPa"}, {"OutletFlux", "1m2/s"}, {"InletFlux", "1m2/s"}, {"Rho", "kg/m3"}, {"U", "m/s"}};
   static const std::map<std::string, const char*> d3q19 = {
       {"nu", "1m2/s"},    {"InletVelocity", "1m/s"}, {"InletPressure", "1Pa"}, {"InletDensity", "1kg/m3"},
       {"Flux", "m3/s"},   {"XYvx", "m3/s"},          {"XYvy", "m3/s"},         {"XYvz", "m3/s"},
@@ -264,10 +265,11 @@ const char* quantity_unit(int model, const std::string& name) {
       {"YZvy", "m3/s"},   {"YZvz", "m3/s"},          {"YZrho", "kg/m"},        {"YZarea", "m2"},
       {"VOLvx", "m4/s"},  {"VOLvy", "m4/s"},         {"VOLvz", "m4/s"},        {"VOLpx", "mkg/s"},
       {"VOLpy", "mkg/s"}, {"VOLpz", "mkg/s"},        {"VOLrho", "kg"},         {"VOLvolume", "m3"},
-      {"MaxV", "m3"}};
+      {"MaxV", "m3"},     {"P", "Pa"},               {"U", "m/s"}};
   static const std::map<std::string, const char*> d3q27c = {
       {"Density", "kg/m3"}, {"Flux", "m3/s"}, {"Drag", "N"},         {"Lift", "N"},         {"Lateral", "N"},
-      {"Mass", "kg"},       {"XMomentum", "kgm/s"}, {"YMomentum", "kgm/s"}, {"ZMomentum", "kgm/s"}};
+      {"Mass", "kg"},       {"XMomentum", "kgm/s"}, {"YMomentum", "kgm/s"}, {"ZMomentum", "kgm/s"},
+      {"P", "Pa"},          {"U", "m/s"}};
   const std::map<std::string, const char*>& m = model == MODEL_D2Q9 ? d2q9 : (model == MODEL_D3Q19 ? d3q19 : d3q27c);
   const auto it = m.find(name);
   return it == m.end() ? "1" : it->second;
@@ -276,6 +278,22 @@ const char* quantity_unit(int model, const std::string& name) {
 // Multiplier from a lattice value to SI for the Log's _si columns
 // (LogScales, src/Solver.cpp.Rt:145-159): 1 / (lattice value of one unit).
 double si_scale(int model, const std::string& name) { return 1.0 / g_units.alt(quantity_unit(model, name)); }
+
+// Base64 (RFC 4648) of n bytes, '=' padded, no line breaks.
+void put_base64(FILE* o, const void* data, size_t n) {
+  static const char* A = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
+  const unsigned char* b = static_cast<const unsigned char*>(data);
+  std::string out;
+  out.reserve((n + 2) / 3 * 4);
+  for (size_t i = 0; i < n; i += 3) {
+    const unsigned w = (unsigned)b[i] << 16 | (i + 1 < n ? (unsigned)b[i + 1] << 8 : 0u) | (i + 2 < n ? b[i + 2] : 0u);
+    out += A[w >> 18 & 63];
+    out += A[w >> 12 & 63];
+    out += i + 1 < n ? A[w >> 6 & 63] : '=';
+    out += i + 2 < n ? A[w & 63] : '=';
+  }
+  std::fwrite(out.data(), 1, out.size(), o);
+}
 
 int parse_int(const std::string& s) { return (int)std::lround(parse_value(s)); }
 
@@ -668,6 +686,116 @@ struct Runner {
     std::fprintf(o, "\n");
     std::fclose(o);
   }
+  // <VTK> (src/Handlers/cbVTK.cpp, src/vtkLattice.cpp:9-56, src/vtkOutput.cpp):
+  // a VTK XML ImageData file <case>_<name>_P00_<iteration>.vti with cell data
+  // of the region (dx..nz attributes, default the whole lattice), and the
+  // parallel wrapper .pvti naming it as its one piece. Fields: "flag" (the
+  // node-type word) when named in `what`; each node-type group and
+  // SETTINGZONE as UInt8 (the group's bits); each quantity in SI units
+  // (1 / lattice value of its unit). `what` is a comma list of names, default
+  // "all" (every group and quantity). Arrays are inline base64: a 4-byte
+  // length block, then the data block.
+  void write_vtk(const Callback& c) {
+    int tot[3];
+    tclb_get_size(lat, &tot[0], &tot[1], &tot[2]);
+    int reg[6] = {0, 0, 0, tot[0], tot[1], tot[2]};  // x0 y0 z0 nx ny nz
+    const char* dn[3] = {"dx", "dy", "dz"};
+    const char* nn[3] = {"nx", "ny", "nz"};
+    for (int a = 0; a < 3; a++) {
+      if (const std::string* v = c.node->attr(dn[a])) {
+        reg[a] = parse_int(*v);
+        if (reg[a] < 0) {  // from the far face
+          reg[a] += tot[a];
+          reg[3 + a] = tot[a] - reg[a];
+        }
+      }
+      if (const std::string* v = c.node->attr(nn[a])) {
+        reg[3 + a] = parse_int(*v);
+        if (reg[3 + a] < 0) reg[3 + a] += tot[a] - reg[a];
+      }
+      const int lo = std::max(0, reg[a]), hi = std::min(tot[a], reg[a] + reg[3 + a]);
+      reg[a] = lo;
+      reg[3 + a] = std::max(0, hi - lo);
+    }
+    const size_t size = (size_t)reg[3] * reg[4] * reg[5];
+    if (size == 0) throw CaseError("<VTK> region is empty");
+    bool all = false;
+    std::vector<std::string> what;
+    {
+      std::stringstream ss(c.node->attr_or("what", "all"));
+      std::string w;
+      while (std::getline(ss, w, ','))
+        if (w == "all") all = true;
+        else what.push_back(w);
+    }
+    auto named = [&](const std::string& n) { return std::find(what.begin(), what.end(), n) != what.end(); };
+    const std::string name = c.node->attr_or("name", "VTK");
+    const std::string fn = iter_file(name, ".vti"), pfn = iter_file(name, ".pvti");
+    FILE* o = std::fopen(fn.c_str(), "wb");
+    FILE* po = std::fopen(pfn.c_str(), "wb");
+    if (!o || !po) {
+      if (o) std::fclose(o);
+      if (po) std::fclose(po);
+      throw CaseError("cannot write " + fn);
+    }
+    const double spacing = 1.0 / g_units.alt("m");
+    char ext[160];
+    std::snprintf(ext, sizeof(ext), "%d %d %d %d %d %d", reg[0], reg[0] + reg[3], reg[1], reg[1] + reg[4], reg[2],
+                  reg[2] + reg[5]);
+    std::fprintf(o, "<?xml version=\"1.0\"?>\n<VTKFile type=\"ImageData\" version=\"0.1\" byte_order=\"LittleEndian\">\n");
+    std::fprintf(o, "<ImageData WholeExtent=\"%s\" Origin=\"0 0 0\" Spacing=\"%lg %lg %lg\">\n", ext, spacing, spacing,
+                 spacing);
+    std::fprintf(o, "<Piece Extent=\"%s\">\n<CellData Scalars=\"rho\" Vectors=\"velocity\">\n", ext);
+    std::fprintf(po, "<?xml version=\"1.0\"?>\n<VTKFile type=\"PImageData\" version=\"0.1\" byte_order=\"LittleEndian\">\n");
+    std::fprintf(po, "<PImageData WholeExtent=\"%s\" Origin=\"0 0 0\" Spacing=\"%lg %lg %lg\">\n", ext, spacing,
+                 spacing, spacing);
+    const size_t sl = fn.find_last_of('/');
+    std::fprintf(po, "<Piece Extent=\"%s\" Source=\"%s\"/>\n<PCellData Scalars=\"rho\" Vectors=\"velocity\">\n", ext,
+                 (sl == std::string::npos ? fn : fn.substr(sl + 1)).c_str());
+    auto field = [&](const char* fname, const char* type, int comps, const void* data, size_t bytes) {
+      std::fprintf(o, "<DataArray type=\"%s\" Name=\"%s\" format=\"binary\" encoding=\"base64\" NumberOfComponents=\"%d\">\n",
+                   type, fname, comps);
+      const int len = (int)bytes;
+      put_base64(o, &len, sizeof(len));
+      put_base64(o, data, bytes);
+      std::fprintf(o, "\n</DataArray>\n");
+      std::fprintf(po, "<PDataArray type=\"%s\" Name=\"%s\" format=\"binary\" encoding=\"base64\" NumberOfComponents=\"%d\"/>\n",
+                   type, fname, comps);
+    };
+    // node types of the region
+    std::vector<uint16_t> all_fl((size_t)tot[0] * tot[1] * tot[2]), fl(size);
+    ck(tclb_get_flags(lat, all_fl.data()), "flags");
+    size_t k = 0;
+    for (int z = 0; z < reg[5]; z++)
+      for (int y = 0; y < reg[4]; y++)
+        for (int x = 0; x < reg[3]; x++)
+          fl[k++] = all_fl[(size_t)(reg[0] + x) + (size_t)tot[0] * ((size_t)(reg[1] + y) + (size_t)tot[1] * (reg[2] + z))];
+    if (named("flag")) field("flag", "UInt16", 1, fl.data(), size * 2);
+    std::vector<unsigned char> small(size);
+    for (int gi = 0; gi <= T->ngroups; gi++) {  // the model's groups, then SETTINGZONE
+      const bool zone = gi == T->ngroups;
+      const std::string gname = zone ? "SETTINGZONE" : T->group_names[gi];
+      if (!all && !named(gname)) continue;
+      const unsigned mask = zone ? (0xFFFFu << T->zone_shift) & 0xFFFFu : (unsigned)T->group_masks[gi];
+      int shift = 0;
+      while (shift < 16 && !(mask >> shift & 1u)) shift++;
+      for (size_t i = 0; i < size; i++) small[i] = (unsigned char)((fl[i] & mask) >> shift);
+      field(gname.c_str(), "UInt8", 1, small.data(), size);
+    }
+    const size_t rs = precision == TCLB_FP64 ? 8 : 4;
+    for (int q = 0; q < T->nquantities; q++) {
+      if (!all && !named(T->quantity_names[q])) continue;
+      const int comp = T->quantity_vector[q] ? 3 : 1;
+      std::vector<char> buf(size * comp * rs);
+      ck(tclb_get_quantity(lat, q, reg, buf.data(), si_scale(model, T->quantity_names[q]), nullptr), "quantity");
+      field(T->quantity_names[q], rs == 8 ? "Float64" : "Float32", comp, buf.data(), buf.size());
+    }
+    std::fprintf(o, "</CellData>\n</Piece>\n</ImageData>\n</VTKFile>\n");
+    std::fprintf(po, "</PCellData>\n</PImageData>\n</VTKFile>\n");
+    std::fclose(o);
+    std::fclose(po);
+  }
+
   // binWriteLattice (src/vtkLattice.cpp:58-81): one raw real_t file per quantity
   void write_bin(const std::string& prefix) {
     int nx, ny, nz;
@@ -859,6 +987,7 @@ struct Runner {
   // returns true to stop the solve
   bool do_callback(Callback& c) {
     if (c.kind == "Stop") return stop_check(c);
+    if (c.kind == "VTK") write_vtk(c);
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
@@ -917,11 +1046,11 @@ struct Runner {
       else if (n->name == "Init") init();
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
-               n->name == "Stop")
+               n->name == "Stop" || n->name == "VTK")
         callback(n);
       else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)
-      } else if (n->name == "VTK" || n->name == "TXT" || n->name == "Average") {
+      } else if (n->name == "TXT" || n->name == "Average") {
         if (verbose) std::printf("[tclb_run] <%s> is not supported; skipped\n", n->name.c_str());
       } else {
         throw CaseError("unsupported element <" + n->name + ">");

@@ -186,6 +186,62 @@ def test_stop_ends_the_solve(tmp_path):
     assert its is None and "Stop" in err
 
 
+def read_vti(path):
+    """Cell arrays of a VTK XML ImageData file with inline base64 arrays (a
+    4-byte length block, then the data block) -> {name: array}, spacing."""
+    import base64
+    import xml.etree.ElementTree as ET
+
+    root = ET.parse(path).getroot()
+    img = root.find("ImageData")
+    spacing = [float(v) for v in img.get("Spacing").split()]
+    types = {"Float32": np.float32, "Float64": np.float64, "UInt8": np.uint8, "UInt16": np.uint16}
+    out = {}
+    for da in img.iter("DataArray"):
+        text = da.text.strip()
+        n = np.frombuffer(base64.b64decode(text[:8]), np.int32)[0]
+        data = np.frombuffer(base64.b64decode(text[8:]), types[da.get("type")])
+        assert data.nbytes == n
+        out[da.get("Name")] = data.reshape(-1, int(da.get("NumberOfComponents")))
+    return out, spacing
+
+
+@pytest.mark.gpu
+def test_vtk_output(tmp_path):
+    """<VTK> writes the quantities in SI units, the node-type groups and,
+    when named, the raw node types; with no gauges SI is the lattice value."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    got = {}
+    for name in ("channel_disc", "channel_disc_si"):
+        text = open(os.path.join(HERE, "cases", name + ".xml")).read()
+        text = text.replace("<BIN ", '<VTK Iterations="%s"/><VTK name="part" what="U,BOUNDARY,flag" dx="10" nx="20" '
+                                     'Iterations="%s"/><BIN ' % (("200", "200") if name == "channel_disc" else ("4s", "4s")))
+        path = tmp_path / (name + ".xml")
+        path.write_text(text)
+        out = str(tmp_path / name) + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert os.path.exists(out + name + "_VTK_P00_00000200.pvti")
+        got[name] = (read_vti(out + name + "_VTK_P00_00000200.vti"), read_vti(out + name + "_part_P00_00000200.vti"),
+                     np.fromfile(out + name + "_BIN_P00_00000200.U.bin", np.float32).reshape(-1, 3))
+    (full, sp), (part, _), u_bin = got["channel_disc"]
+    assert sp == [1.0, 1.0, 1.0]
+    assert set(full) == {"BOUNDARY", "COLLISION", "OBJECTIVE", "SETTINGZONE", "Rho", "U"}
+    assert np.array_equal(full["U"], u_bin)
+    fl = case_geometry(open(os.path.join(HERE, "cases", "channel_disc.xml")).read(), "d2q9")
+    assert np.array_equal(full["BOUNDARY"][:, 0], (fl & 0xF).ravel())
+    assert set(part) == {"U", "BOUNDARY", "flag"}
+    nz, ny, nx = fl.shape
+    assert np.array_equal(part["flag"][:, 0], fl[:, :, 10:30].ravel())
+    assert np.array_equal(part["U"], u_bin.reshape(ny, nx, 3)[:, 10:30].reshape(-1, 3))
+    (full_si, sp_si), _, u_bin_si = got["channel_disc_si"]
+    assert sp_si == pytest.approx([1e-3] * 3)
+    # 1 lattice velocity = 1 mm per 1/50 s = 0.05 m/s
+    assert full_si["U"][:, 0] == pytest.approx(u_bin_si[:, 0] * 0.05, rel=1e-5, abs=1e-12)
+
+
 @pytest.mark.gpu
 def test_case_file_run_matches_api(tmp_path):
     """tclb_run on the channel case: the Log CSV rows and the final BIN files
