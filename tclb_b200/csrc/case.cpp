@@ -796,6 +796,63 @@ struct Runner {
     std::fclose(po);
   }
 
+  // <TXT> (src/Handlers/cbTXT.cpp, txtWriteLattice src/vtkLattice.cpp:83-161):
+  // <case>_<name>_P00_<iteration>_info.txt with the SI sizes of the lattice
+  // units and the lattice size, and one text file per quantity (`what`,
+  // default all) in SI units: %.8g (float) or %.16lg (double) values, a new
+  // line after every nx nodes. Vector quantities give x y z per node (TCLB
+  // reads them into a one-value-per-node buffer). gzip="true" pipes each
+  // quantity file through gzip into <file>.gz.
+  void write_txt(const Callback& c) {
+    int nx, ny, nz;
+    tclb_get_size(lat, &nx, &ny, &nz);
+    const size_t size = (size_t)nx * ny * nz;
+    const std::string base = iter_file(c.node->attr_or("name", "TXT"), "");
+    const std::string gz = c.node->attr_or("gzip", "false");
+    const bool gzip = gz == "true" || gz == "1" || gz == "yes";
+    bool all = false;
+    std::vector<std::string> what;
+    {
+      std::stringstream ss(c.node->attr_or("what", "all"));
+      std::string w;
+      while (std::getline(ss, w, ','))
+        if (w == "all") all = true;
+        else what.push_back(w);
+    }
+    {
+      FILE* f = std::fopen((base + "_info.txt").c_str(), "w");
+      if (!f) throw CaseError("cannot write " + base + "_info.txt");
+      std::fprintf(f, "dx: %lg\ndt: %lg\ndm: %lg\ndT: %lg\n", 1.0 / g_units.alt("m"), 1.0 / g_units.alt("s"),
+                   1.0 / g_units.alt("kg"), 1.0 / g_units.alt("K"));
+      std::fprintf(f, "size: %zu\nNX: %d\nNY: %d\nNZ: %d\n", size, nx, ny, nz);
+      std::fclose(f);
+    }
+    const bool dbl = precision == TCLB_FP64;
+    for (int q = 0; q < T->nquantities; q++) {
+      const std::string qn = T->quantity_names[q];
+      if (!all && std::find(what.begin(), what.end(), qn) == what.end()) continue;
+      const int comp = T->quantity_vector[q] ? 3 : 1;
+      std::vector<char> buf(size * comp * (dbl ? 8 : 4));
+      ck(tclb_get_quantity(lat, q, nullptr, buf.data(), si_scale(model, qn), nullptr), "quantity");
+      const std::string fn = base + "_" + qn + ".txt";
+      FILE* f = gzip ? popen(("gzip > '" + fn + ".gz'").c_str(), "w") : std::fopen(fn.c_str(), "w");
+      if (!f) throw CaseError("cannot write " + fn);
+      for (size_t i = 0; i < size; i++) {
+        for (int k = 0; k < comp; k++) {
+          if (k) std::fputc(' ', f);
+          if (dbl) std::fprintf(f, "%.16lg", reinterpret_cast<const double*>(buf.data())[i * comp + k]);
+          else std::fprintf(f, "%.8g", (double)reinterpret_cast<const float*>(buf.data())[i * comp + k]);
+        }
+        std::fputc((i + 1) % nx == 0 ? '\n' : ' ', f);
+      }
+      if (gzip) {
+        if (pclose(f) != 0) throw CaseError("gzip failed for " + fn);
+      } else {
+        std::fclose(f);
+      }
+    }
+  }
+
   // binWriteLattice (src/vtkLattice.cpp:58-81): one raw real_t file per quantity
   void write_bin(const std::string& prefix) {
     int nx, ny, nz;
@@ -988,6 +1045,7 @@ struct Runner {
   bool do_callback(Callback& c) {
     if (c.kind == "Stop") return stop_check(c);
     if (c.kind == "VTK") write_vtk(c);
+    if (c.kind == "TXT") write_txt(c);
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
@@ -1046,11 +1104,11 @@ struct Runner {
       else if (n->name == "Init") init();
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
-               n->name == "Stop" || n->name == "VTK")
+               n->name == "Stop" || n->name == "VTK" || n->name == "TXT")
         callback(n);
       else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)
-      } else if (n->name == "TXT" || n->name == "Average") {
+      } else if (n->name == "Average") {
         if (verbose) std::printf("[tclb_run] <%s> is not supported; skipped\n", n->name.c_str());
       } else {
         throw CaseError("unsupported element <" + n->name + ">");

@@ -243,6 +243,33 @@ def test_vtk_output(tmp_path):
 
 
 @pytest.mark.gpu
+def test_txt_output(tmp_path):
+    """<TXT>: the info file and one text file per quantity (SI units; rows of
+    nx nodes; vectors x y z per node), the same values as the BIN files."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    text = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    text = text.replace("<BIN ", '<TXT Iterations="200"/><BIN ')
+    path = tmp_path / "case.xml"
+    path.write_text(text)
+    out = str(tmp_path / "out") + "/"
+    r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    base = out + "case_TXT_P00_00000200"
+    info = dict(line.split(": ") for line in open(base + "_info.txt").read().strip().splitlines())
+    assert info["NX"] == "256" and info["NY"] == "64" and info["NZ"] == "1" and float(info["dx"]) == 1.0
+    rho = np.loadtxt(base + "_Rho.txt")
+    assert rho.shape == (64, 256)
+    rho_bin = np.fromfile(out + "case_BIN_P00_00000200.Rho.bin", np.float32).reshape(64, 256)
+    assert np.allclose(rho, rho_bin, rtol=1e-7, atol=0)
+    u = np.loadtxt(base + "_U.txt")
+    assert u.shape == (64, 256 * 3)
+    u_bin = np.fromfile(out + "case_BIN_P00_00000200.U.bin", np.float32).reshape(64, 256 * 3)
+    assert np.allclose(u, u_bin, rtol=1e-7, atol=1e-30)
+
+
+@pytest.mark.gpu
 def test_case_file_run_matches_api(tmp_path):
     """tclb_run on the channel case: the Log CSV rows and the final BIN files
     equal what the Python API produces for the same flags and settings."""
