@@ -1109,7 +1109,11 @@ struct Runner {
       else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)
       } else if (n->name == "Average") {
-        if (verbose) std::printf("[tclb_run] <%s> is not supported; skipped\n", n->name.c_str());
+        // cbAveraging (src/Handlers/cbAveraging.cpp:5-16) zeroes the densities a
+        // model declares average=TRUE and restarts the averaging count. Only the
+        // AVG option of d3q27_cumulant (models/flow/d3q27_cumulant/Dynamics.R:66-90)
+        // declares any; the plain d2q9, d3q19 and d3q27_cumulant have none, so
+        // there is nothing to reset.
       } else {
         throw CaseError("unsupported element <" + n->name + ">");
       }
