@@ -474,6 +474,57 @@ struct Geometry {
           for (int y = r.dy - 1; y < r.dy + r.ny + 1; y++)
             for (int z = r.dz - 1; z < r.dz + r.nz + 1; z++)
               if (in_sphere((.5 + x - r.dx) / r.nx, (.5 + y - r.dy) / r.ny, 0.5)) dot(x, y, z);
+      } else if (n->name == "Pipe" || n->name == "PipeY" || n->name == "PipeZ") {
+        // (:1022-1052) the region outside the cylinder inscribed in the box, axis
+        // along x (Pipe), y (PipeY) or z (PipeZ); one extra layer across the axis
+        const int ax = n->name == "Pipe" ? 0 : n->name == "PipeY" ? 1 : 2;
+        const int lo[3] = {r.dx - (ax != 0), r.dy - (ax != 1), r.dz - (ax != 2)};
+        const int hi[3] = {r.dx + r.nx + (ax != 0), r.dy + r.ny + (ax != 1), r.dz + r.nz + (ax != 2)};
+        for (int x = lo[0]; x < hi[0]; x++)
+          for (int y = lo[1]; y < hi[1]; y++)
+            for (int z = lo[2]; z < hi[2]; z++) {
+              const double fx = (.5 + x - r.dx) / r.nx, fy = (.5 + y - r.dy) / r.ny, fz = (.5 + z - r.dz) / r.nz;
+              const bool in = ax == 0 ? in_sphere(0.5, fy, fz) : ax == 1 ? in_sphere(0.5, fx, fz) : in_sphere(0.5, fy, fx);
+              if (!in) dot(x, y, z);
+            }
+      } else if (n->name == "OffgridPipe" || n->name == "XPipe" || n->name == "YPipe" || n->name == "ZPipe" ||
+                 n->name == "XAnnulus") {
+        // (:835-1021) elliptic cylinders about an off-grid centre (x, y, z), the
+        // axis z (OffgridPipe, ZPipe), x (XPipe, XAnnulus) or y (YPipe). Across
+        // the axis the box spans the radii plus 5 nodes, truncated to int;
+        // along it the element's region. YPipe and ZPipe measure the x offset
+        // from y (.5 + x - y0), as TCLB does. XAnnulus keeps the nodes inside
+        // the outer ellipse (Ro or Ry_o/Rz_o) and outside the inner one.
+        const double c[3] = {parse_value(n->attr_or("x", "0")), parse_value(n->attr_or("y", "0")),
+                             parse_value(n->attr_or("z", "0"))};
+        const int ax = n->name == "XPipe" || n->name == "XAnnulus" ? 0 : n->name == "YPipe" ? 1 : 2;
+        const int a = ax == 0 ? 1 : 0, b = ax == 2 ? 1 : 2;  // cross-section axes, a < b
+        const char* nm = "xyz";
+        const double ca = (n->name == "YPipe" || n->name == "ZPipe") ? c[1] : c[a], cb = c[b];
+        const bool annulus = n->name == "XAnnulus";
+        auto radius = [&](const std::string& k, const char* all) {
+          if (n->attr(all)) return parse_value(*n->attr(all));
+          return parse_value(n->attr_or(k, "0"));
+        };
+        double Ra, Rb, Ra_i = 0, Rb_i = 0;
+        if (annulus) {
+          Ra = radius("Ry_o", "Ro"), Rb = radius("Rz_o", "Ro");
+          Ra_i = radius("Ry_i", "Ri"), Rb_i = radius("Rz_i", "Ri");
+        } else {
+          Ra = radius(std::string("R") + nm[a], "R"), Rb = radius(std::string("R") + nm[b], "R");
+        }
+        int lo[3] = {r.dx, r.dy, r.dz}, len[3] = {r.nx, r.ny, r.nz};
+        lo[a] = (int)(c[a] - Ra - 5), len[a] = (int)(2 * Ra + 10);
+        lo[b] = (int)(c[b] - Rb - 5), len[b] = (int)(2 * Rb + 10);
+        for (int x = lo[0]; x < lo[0] + len[0]; x++)
+          for (int y = lo[1]; y < lo[1] + len[1]; y++)
+            for (int z = lo[2]; z < lo[2] + len[2]; z++) {
+              const int p[3] = {x, y, z};
+              const double pa = .5 + p[a] - ca, pb = .5 + p[b] - cb;
+              bool in = pa * pa / (Ra * Ra) + pb * pb / (Rb * Rb) < 1.;
+              if (annulus) in = in && pa * pa / (Ra_i * Ra_i) + pb * pb / (Rb_i * Rb_i) > 1.;
+              if (in) dot(x, y, z);
+            }
       } else if (n->name == "Wedge") {
         const std::string dir = n->attr_or("direction", "");
         for (int x = r.dx; x < r.dx + r.nx; x++)

@@ -84,6 +84,74 @@ def test_wedge_and_units():
     assert fl[0, 0, 0] == M.get("d2q9").flag("Solid")  # 20mm -> 0.02 -> column 0, 1m -> nx=1
 
 
+def test_pipes():
+    """<Pipe>, <PipeY>, <PipeZ>: every node of the box (grown by one layer across
+    the axis, clipped to the lattice) outside the inscribed circle of the cross
+    section, (2u-1)^2 + (2v-1)^2 >= 1 with u, v the node centres over the box."""
+    wall = M.get("d3q19").flag("Wall")
+    box = dict(dx=3, nx=10, dy=2, ny=8, dz=1, nz=6)
+    for name, axis in (("Pipe", 0), ("PipeY", 1), ("PipeZ", 2)):
+        attrs = " ".join(f'{k}="{v}"' for k, v in box.items())
+        fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="12" nz="10"><Wall><{name} {attrs}/></Wall>'
+                           '</Geometry></CLBConfig>', "d3q19")
+        want = np.zeros_like(fl)
+        d = (box["dx"], box["dy"], box["dz"])
+        n = (box["nx"], box["ny"], box["nz"])
+        for z in range(10):
+            for y in range(12):
+                for x in range(32):
+                    c = (x, y, z)
+                    grow = [0 if a == axis else 1 for a in range(3)]
+                    if not all(d[a] - grow[a] <= c[a] < d[a] + n[a] + grow[a] for a in range(3)):
+                        continue
+                    u = [(0.5 + c[a] - d[a]) / n[a] for a in range(3) if a != axis]
+                    if (2 * u[0] - 1) ** 2 + (2 * u[1] - 1) ** 2 >= 1:
+                        want[z, y, x] = wall
+        assert np.array_equal(fl, want), name
+        assert (fl != 0).any() and (fl == 0).any(), name
+
+
+def test_offgrid_pipes():
+    """<OffgridPipe>/<ZPipe> (axis z), <XPipe>, <YPipe> and <XAnnulus>: nodes whose
+    centres lie inside the ellipse about the off-grid centre, over a box of the
+    radii + 5 nodes across the axis. YPipe and ZPipe take the x offset from y
+    (TCLB's .5 + x - y0), so their x centre is y."""
+    wall = M.get("d3q19").flag("Wall")
+    X, Y, Z = 64, 24, 20  # nx a multiple of 32 (no padding)
+
+    def want(axis, c, R, Ri=None, ca=None):
+        a, b = [k for k in range(3) if k != axis]
+        out = np.zeros((Z, Y, X), np.uint16)
+        lo = [int(c[k] - R[k] - 5) if k != axis else 0 for k in range(3)]
+        hi = [lo[k] + int(2 * R[k] + 10) if k != axis else (X, Y, Z)[k] for k in range(3)]
+        ca = c[a] if ca is None else ca
+        for z in range(max(lo[2], 0), min(hi[2], Z)):
+            for y in range(max(lo[1], 0), min(hi[1], Y)):
+                for x in range(max(lo[0], 0), min(hi[0], X)):
+                    p = (x, y, z)
+                    pa, pb = 0.5 + p[a] - ca, 0.5 + p[b] - c[b]
+                    inside = pa * pa / R[a] ** 2 + pb * pb / R[b] ** 2 < 1
+                    if Ri is not None:
+                        inside = inside and pa * pa / Ri[a] ** 2 + pb * pb / Ri[b] ** 2 > 1
+                    if inside:
+                        out[z, y, x] = wall
+        return out
+
+    c = (17.3, 9.6, 8.2)
+    shapes = [
+        ('<OffgridPipe x="17.3" y="9.6" z="8.2" Rx="6.5" Ry="4.2"/>', want(2, c, (6.5, 4.2, 0))),
+        ('<ZPipe x="17.3" y="9.6" z="8.2" R="5.5"/>', want(2, c, (5.5, 5.5, 0), ca=9.6)),
+        ('<XPipe x="17.3" y="9.6" z="8.2" Ry="6.1" Rz="3.7"/>', want(0, c, (0, 6.1, 3.7))),
+        ('<YPipe x="17.3" y="9.6" z="8.2" Rx="4.4" Rz="5.2"/>', want(1, c, (4.4, 0, 5.2), ca=9.6)),
+        ('<XAnnulus x="17.3" y="9.6" z="8.2" Ro="7.5" Ri="4"/>', want(0, c, (0, 7.5, 7.5), Ri=(0, 4, 4))),
+    ]
+    for elem, ref in shapes:
+        fl = case_geometry(f'<CLBConfig><Geometry nx="{X}" ny="{Y}" nz="{Z}"><Wall>{elem}</Wall></Geometry></CLBConfig>',
+                           "d3q19")
+        assert fl.shape == ref.shape and np.array_equal(fl, ref), elem
+        assert (fl != 0).any(), elem
+
+
 def test_bad_case_is_an_error_not_an_exit():
     lib = load_library()
     lib.tclb_case_last_error.restype = ctypes.c_char_p
