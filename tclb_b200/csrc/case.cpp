@@ -431,6 +431,232 @@ struct Geometry {
       if (const XmlNode* z = defaults->child_by_attr("Zone", "name", name)) return z;
     return nullptr;
   }
+  // <STL> (Geometry::transformSTL :381-473, Geometry::loadSTL :507-687): a
+  // binary STL file whose vertices (float, as stored in the file) are rotated
+  // by Xrot, Yrot, Zrot in turn, scaled by `scale`, moved by x, y, z, rounded
+  // to 1e-5 and moved by -0.5 plus a small per-axis offset, so node centres
+  // do not fall on faces. side="in" (default) or "out": rays along ray_axis
+  // (default y) from the start of the element's region; a node of the region
+  // is drawn when the number of faces at or above it is odd (in) or even
+  // (out). side="surface": a node is drawn when the link to any of its 26
+  // neighbours crosses a face (TCLB also records the cut fractions, which only
+  // interpolated bounce-back models read; a link parallel to a face is no cut).
+  void draw_stl(const XmlNode* n, const Region& reg) {
+    const std::string* file = n->attr("file");
+    if (!file) throw CaseError("<STL> needs a file attribute");
+    int inside_out = 0, axis = 1;
+    if (const std::string* s = n->attr("side")) {
+      if (*s == "in") inside_out = 0;
+      else if (*s == "out") inside_out = 1;
+      else if (*s == "surface") inside_out = 2;
+      else throw CaseError("<STL> side must be in, out or surface");
+    }
+    if (const std::string* s = n->attr("ray_axis")) {
+      if (inside_out == 2) throw CaseError("<STL> ray_axis applies to side in or out only");
+      if (*s == "x") axis = 0;
+      else if (*s == "y") axis = 1;
+      else if (*s == "z") axis = 2;
+      else throw CaseError("<STL> ray_axis must be x, y or z");
+    }
+    std::ifstream in(*file, std::ios::binary);
+    if (!in) throw CaseError("cannot open " + *file);
+    char header[80];
+    uint32_t ntri = 0;
+    in.read(header, 80);
+    in.read(reinterpret_cast<char*>(&ntri), 4);
+    if (!in) throw CaseError(*file + " is not a binary STL file");
+    if (std::strncmp(header, "solid", 5) == 0) throw CaseError(*file + " is not in binary STL format");
+    struct Tri { float p[3][3]; };
+    std::vector<Tri> tri(ntri);
+    for (uint32_t i = 0; i < ntri; i++) {
+      char rec[50];  // normal, three vertices (float x 12), attribute (uint16)
+      in.read(rec, 50);
+      if (!in) throw CaseError(*file + " ended while reading its triangles");
+      std::memcpy(tri[i].p, rec + 12, 36);
+    }
+    static const char* rot[3] = {"Xrot", "Yrot", "Zrot"};
+    for (int d = 0; d < 3; d++) {
+      const std::string* a = n->attr(rot[d]);
+      if (!a) continue;
+      const double v = parse_value(*a);
+      const int i1 = (d + 1) % 3, i2 = (d + 2) % 3;
+      for (auto& t : tri)
+        for (auto& p : t.p) {
+          const double y = p[i1], z = p[i2];
+          p[i1] = (float)(std::cos(v) * y - std::sin(v) * z);
+          p[i2] = (float)(std::sin(v) * y + std::cos(v) * z);
+        }
+    }
+    if (const std::string* a = n->attr("scale")) {
+      const double v = parse_value(*a);
+      for (auto& t : tri)
+        for (auto& p : t.p)
+          for (float& c : p) c = (float)(v * c);
+    }
+    static const char* mv[3] = {"x", "y", "z"};
+    for (int j = 0; j < 3; j++)
+      if (const std::string* a = n->attr(mv[j])) {
+        const double v = parse_value(*a);
+        for (auto& t : tri)
+          for (auto& p : t.p) p[j] = (float)(p[j] + v);
+      }
+    static const double perturb[3] = {0.1403e-4, 0.1687e-4, 0.1987e-4};
+    auto round_int = [](double v) { return v > 0 ? (int)(v + 0.5) : (int)(v - 0.5); };
+    for (auto& t : tri)
+      for (auto& p : t.p)
+        for (int j = 0; j < 3; j++) {
+          p[j] = (float)(round_int(p[j] * 1e5) * 1e-5);
+          p[j] = (float)(p[j] + (perturb[j] - 0.5));
+        }
+    const int rlo[3] = {reg.dx, reg.dy, reg.dz}, rn[3] = {reg.nx, reg.ny, reg.nz};
+    std::vector<int> lev;
+    if (inside_out != 2) lev.assign((size_t)reg.nx * reg.ny * reg.nz, inside_out);
+    for (const Tri& t : tri) {
+      int lo[3], hi[3];
+      for (int j = 0; j < 3; j++) {
+        lo[j] = (int)std::ceil(t.p[0][j]);
+        if (t.p[1][j] < lo[j]) lo[j] = (int)std::ceil(t.p[1][j]);
+        if (t.p[2][j] < lo[j]) lo[j] = (int)std::ceil(t.p[2][j]);
+        hi[j] = (int)std::floor(t.p[0][j]);
+        if (t.p[1][j] > hi[j]) hi[j] = (int)std::floor(t.p[1][j]);
+        if (t.p[2][j] > hi[j]) hi[j] = (int)std::floor(t.p[2][j]);
+        lo[j] -= 1;
+        hi[j] += 1;
+      }
+      if (inside_out == 2) {
+        for (int x = lo[0]; x <= hi[0]; x++)
+          for (int z = lo[2]; z <= hi[2]; z++)
+            for (int y = lo[1]; y <= hi[1]; y++) {
+              if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) continue;
+              for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                  for (int dx = -1; dx <= 1; dx++)
+                    if ((dx || dy || dz) && link_cuts(t.p, x, y, z, dx, dy, dz)) dot(x, y, z);
+            }
+        continue;
+      }
+      const int a1 = axis, a2 = (axis + 1) % 3, a3 = (axis + 2) % 3;
+      const double v1[2] = {(double)(float)(t.p[1][a2] - t.p[0][a2]), (double)(float)(t.p[1][a3] - t.p[0][a3])};
+      const double v2[2] = {(double)(float)(t.p[2][a2] - t.p[0][a2]), (double)(float)(t.p[2][a3] - t.p[0][a3])};
+      const double c0 = v1[0] * v2[1] - v1[1] * v2[0];
+      const double dv[2] = {-0.5694552, 0.8220224};  // fixed direction resolving hits on an edge
+      const double dc1 = (v1[0] * dv[1] - v1[1] * dv[0]) / c0, dc2 = (dv[0] * v2[1] - dv[1] * v2[0]) / c0;
+      const double dc3 = -dc1 - dc2;
+      for (int x2 = lo[a2]; x2 <= hi[a2]; x2++)
+        for (int x3 = lo[a3]; x3 <= hi[a3]; x3++) {
+          const double v[2] = {(double)((float)x2 - t.p[0][a2]), (double)((float)x3 - t.p[0][a3])};
+          const double c1 = (v1[0] * v[1] - v1[1] * v[0]) / c0, c2 = (v[0] * v2[1] - v[1] * v2[0]) / c0;
+          const double c3 = 1. - c1 - c2;
+          int topo = 0;
+          topo += c1 == 0 ? dc1 > 0 : c1 > 0;
+          topo += c2 == 0 ? dc2 > 0 : c2 > 0;
+          topo += c3 == 0 ? dc3 > 0 : c3 > 0;
+          if (topo != 3) continue;
+          const double h = t.p[0][a1] * c3 + t.p[1][a1] * c2 + t.p[2][a1] * c1;
+          int p[3];
+          p[a2] = x2, p[a3] = x3;
+          if (p[a2] < rlo[a2] || p[a2] >= rlo[a2] + rn[a2] || p[a3] < rlo[a3] || p[a3] >= rlo[a3] + rn[a3]) continue;
+          for (int x1 = rlo[a1]; x1 <= h && x1 < rlo[a1] + rn[a1]; x1++) {
+            p[a1] = x1;
+            lev[(size_t)(p[0] - reg.dx) + (size_t)reg.nx * ((size_t)(p[1] - reg.dy) + (size_t)reg.ny * (p[2] - reg.dz))]++;
+          }
+        }
+    }
+    if (inside_out == 2) return;
+    for (int x = reg.dx; x < reg.dx + reg.nx; x++)
+      for (int y = reg.dy; y < reg.dy + reg.ny; y++)
+        for (int z = reg.dz; z < reg.dz + reg.nz; z++)
+          if (lev[(size_t)(x - reg.dx) + (size_t)reg.nx * ((size_t)(y - reg.dy) + (size_t)reg.ny * (z - reg.dz))] % 2 == 1)
+            dot(x, y, z);
+  }
+  // calcCut (:479-505): does the link from node (x, y, z) to (x+dx, y+dy, z+dz)
+  // meet the triangle? Solves p1 + s (p2 - p1) + t (p3 - p1) = X + r d by
+  // Cramer's rule; a cut needs s, t, 1 - s - t >= 0 and 0 <= r <= 1.
+  static bool link_cuts(const float (&p)[3][3], int x, int y, int z, int dx, int dy, int dz) {
+    const double X[3] = {(double)x, (double)y, (double)z}, d[3] = {(double)dx, (double)dy, (double)dz};
+    double e1[3], e2[3], w[3], m[3];
+    for (int j = 0; j < 3; j++) {
+      e1[j] = (double)p[1][j] - p[0][j];
+      e2[j] = (double)p[2][j] - p[0][j];
+      w[j] = X[j] - p[0][j];
+      m[j] = -d[j];
+    }
+    auto det = [](const double* a, const double* b, const double* c) {
+      return a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) + a[2] * (b[0] * c[1] - b[1] * c[0]);
+    };
+    const double D = det(e1, e2, m);
+    if (D == 0) return false;
+    const double s = det(w, e2, m) / D, t = det(e1, w, m) / D, r = det(e1, e2, w) / D;
+    return s >= 0 && t >= 0 && 1 - s - t >= 0 && r >= 0 && r <= 1;
+  }
+  // B-spline of order k through the control values p at x in [0, 1]: de Boor's
+  // recursion on clamped uniform knots (src/spline.h:9-41).
+  static double bspline(double x, std::vector<double> p, int k) {
+    const int n = (int)p.size();
+    int i = (int)std::floor(x * (n - k)) + k;
+    if (k > n - 1) k = n - 1;
+    if (i > n - 1) i = n - 1;
+    if (i < k) i = k;
+    auto knot = [&](int j) { return j < k + 1 ? 0.0 : j < n ? 1.0 * (j - k) / (n - k) : 1.0; };
+    for (int j = k; j > 0; j--)
+      for (int l = 0; l < j; l++) {
+        const double a = (x - knot(i - l)) / (knot(i - l + j) - knot(i - l));
+        p[i - l] = a * p[i - l] + (1 - a) * p[i - l - 1];
+      }
+    return p[i];
+  }
+  // <Sweep> (Geometry::loadSweep :689-756): balls moved along the B-spline of
+  // order `order` (default 1) through the <Point x y z r> children, r defaulting
+  // to the element's r (default 1). The curve parameter steps by `step`
+  // (default 1e-4) or 1/`steps`; a ball within 0.25 of the previous one in x, y,
+  // z and r is skipped. A node of the element's region is drawn when its centre
+  // lies in a ball. A step that is not positive is an error (TCLB would loop
+  // for ever).
+  void draw_sweep(const XmlNode* node, const Region& reg) {
+    int order = 1;
+    if (const std::string* a = node->attr("order")) order = std::atoi(a->c_str());
+    double dl = 1e-4;
+    if (const std::string* a = node->attr("step")) dl = std::atof(a->c_str());
+    if (const std::string* a = node->attr("steps")) dl = 1 / parse_value(*a);
+    if (!(dl > 0)) throw CaseError("<Sweep> needs a positive step");
+    double def_r = 1;
+    if (const std::string* a = node->attr("r")) def_r = parse_value(*a);
+    std::vector<double> px, py, pz, pr;
+    for (const auto& c : node->children) {
+      if (c->name != "Point") continue;  // TCLB notes other elements and ignores them
+      px.push_back(parse_value(c->attr_or("x", "0")));
+      py.push_back(parse_value(c->attr_or("y", "0")));
+      pz.push_back(parse_value(c->attr_or("z", "0")));
+      pr.push_back(c->attr("r") ? parse_value(*c->attr("r")) : def_r);
+    }
+    const int n = (int)px.size();
+    if (n == 0) return;
+    if (order > n - 1) order = n - 1;
+    double x0_ = -999.0, y0_ = -999.0, z0_ = -999.0, r0_ = -999.0;
+    for (double l = 0; l < 1; l += dl) {
+      const double x0 = bspline(l, px, order), y0 = bspline(l, py, order), z0 = bspline(l, pz, order),
+                   r = bspline(l, pr, order);
+      if (std::fabs(x0 - x0_) < 0.25 && std::fabs(y0 - y0_) < 0.25 && std::fabs(z0 - z0_) < 0.25 &&
+          std::fabs(r - r0_) < 0.25)
+        continue;
+      x0_ = x0, y0_ = y0, z0_ = z0, r0_ = r;
+      const int b[3] = {(int)(x0 - r - 1), (int)(y0 - r - 1), (int)(z0 - r - 1)}, bn = (int)(2 * r + 2);
+      const int rd[3] = {reg.dx, reg.dy, reg.dz}, rn[3] = {reg.nx, reg.ny, reg.nz};
+      int lo[3], hi[3];
+      bool empty = false;
+      for (int j = 0; j < 3; j++) {
+        lo[j] = std::max(rd[j], b[j]);
+        hi[j] = std::min(rd[j] + rn[j], b[j] + bn);
+        empty = empty || hi[j] <= lo[j];
+      }
+      if (empty) continue;
+      for (int x = lo[0]; x < hi[0]; x++)
+        for (int y = lo[1]; y < hi[1]; y++)
+          for (int z = lo[2]; z < hi[2]; z++)
+            if ((.5 + x - x0) * (.5 + x - x0) + (.5 + y - y0) * (.5 + y - y0) + (.5 + z - z0) * (.5 + z - z0) < r * r)
+              dot(x, y, z);
+    }
+  }
   // Geometry::Draw (:758-1124) for the supported primitives
   void draw(const XmlNode* node) {
     for (const auto& cp : node->children) {
@@ -532,6 +758,10 @@ struct Geometry {
             for (int z = r.dz; z < r.dz + r.nz; z++)
               if (in_wedge((x - r.dx) / (r.nx - 1.), (y - r.dy) / (r.ny - 1.), (z - r.dz) / (r.nz - 1.), dir))
                 dot(x, y, z);
+      } else if (n->name == "STL") {
+        draw_stl(n, r);
+      } else if (n->name == "Sweep") {
+        draw_sweep(n, r);
       } else if (n->name == "Text") {  // node list, x outer, z inner (:1086-1112)
         Region crop = region_of(n->parent);
         const std::string* file = n->attr("file");

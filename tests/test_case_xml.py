@@ -152,6 +152,121 @@ def test_offgrid_pipes():
         assert (fl != 0).any(), elem
 
 
+def write_stl_box(path, lo, hi, header=b"box"):
+    """A closed axis-aligned box as 12 triangles of a binary STL file."""
+    corners = np.array([[(lo, hi)[(i >> k) & 1][k] for k in range(3)] for i in range(8)], np.float32)
+    quads = [(0, 2, 6, 4), (1, 3, 7, 5), (0, 1, 5, 4), (2, 3, 7, 6), (0, 1, 3, 2), (4, 5, 7, 6)]
+    rec = np.zeros(12, dtype=[("n", "<f4", 3), ("p", "<f4", (3, 3)), ("a", "<u2")])
+    for i, (a, b, c, d) in enumerate(quads):
+        rec["p"][2 * i] = corners[[a, b, c]]
+        rec["p"][2 * i + 1] = corners[[a, c, d]]
+    with open(path, "wb") as f:
+        f.write(header.ljust(80, b" "))
+        f.write(np.uint32(12).tobytes())
+        f.write(rec.tobytes())
+
+
+STL_SHIFT = np.array([0.1403e-4, 0.1687e-4, 0.1987e-4]) - 0.5  # node i sits at STL coordinate i + 0.5
+
+
+def stl_inside(shape, lo, hi):
+    """Nodes strictly inside the box [lo, hi] given in STL coordinates."""
+    z, y, x = np.meshgrid(*[np.arange(n) for n in shape], indexing="ij")
+    lo, hi = np.asarray(lo) + STL_SHIFT, np.asarray(hi) + STL_SHIFT
+    return ((x > lo[0]) & (x < hi[0]) & (y > lo[1]) & (y < hi[1]) & (z > lo[2]) & (z < hi[2]))
+
+
+def test_stl_inside_outside(tmp_path):
+    """<STL> side in / out by ray parity along each ray axis, and the rotate /
+    move transform: the nodes of an STL box, and of the same box turned by
+    90 degrees about z and moved in x."""
+    wall = M.get("d3q19").flag("Wall")
+    lo, hi = (3.3, 2.45, 1.65), (11.8, 9.6, 7.15)
+    f = tmp_path / "box.stl"
+    write_stl_box(f, lo, hi)
+    shape = (12, 16, 32)
+    inside = stl_inside(shape, lo, hi)
+    assert inside.sum() == 9 * 8 * 5
+    for extra in ('', ' ray_axis="x"', ' ray_axis="z"'):
+        fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="16" nz="12"><Wall><STL file="{f}"{extra}/></Wall>'
+                           '</Geometry></CLBConfig>', "d3q19")
+        assert np.array_equal(fl == wall, inside), extra
+    fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="16" nz="12"><Wall><STL file="{f}" side="out"/></Wall>'
+                       '</Geometry></CLBConfig>', "d3q19")
+    assert np.array_equal(fl == wall, ~inside)
+    # Zrot turns (x, y) into (-y, x); then x moves by 20
+    fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="16" nz="12"><Wall><STL file="{f}" Zrot="1.5707963267948966" '
+                       'x="20"/></Wall></Geometry></CLBConfig>', "d3q19")
+    turned = stl_inside(shape, (20 - hi[1], lo[0], lo[2]), (20 - lo[1], hi[0], hi[2]))
+    assert turned.sum() == 8 * 9 * 5
+    assert np.array_equal(fl == wall, turned)
+
+
+def test_stl_surface(tmp_path):
+    """<STL side="surface">: the nodes whose link to one of the 26 neighbours
+    crosses the surface of the box (a segment-box slab test)."""
+    wall = M.get("d3q19").flag("Wall")
+    lo, hi = (3.3, 2.45, 1.65), (11.8, 9.6, 7.15)
+    f = tmp_path / "box.stl"
+    write_stl_box(f, lo, hi)
+    fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="16" nz="12"><Wall><STL file="{f}" side="surface"/></Wall>'
+                       '</Geometry></CLBConfig>', "d3q19")
+    blo, bhi = np.asarray(lo) + STL_SHIFT, np.asarray(hi) + STL_SHIFT
+    want = np.zeros((12, 16, 32), bool)
+    dirs = [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1) if dx or dy or dz]
+    for z in range(12):
+        for y in range(16):
+            for x in range(32):
+                X = np.array([x, y, z], float)
+                inside0 = np.all((X > blo) & (X < bhi))
+                for d in dirs:
+                    d = np.array(d, float)
+                    r0, r1 = 0.0, 1.0
+                    for k in range(3):
+                        if d[k] == 0:
+                            if not blo[k] <= X[k] <= bhi[k]:
+                                r0, r1 = 1.0, 0.0
+                        else:
+                            a, b = sorted(((blo[k] - X[k]) / d[k], (bhi[k] - X[k]) / d[k]))
+                            r0, r1 = max(r0, a), min(r1, b)
+                    if r0 <= r1 and not (inside0 and np.all((X + d > blo) & (X + d < bhi))):
+                        want[z, y, x] = True
+                        break
+    assert want.sum() > 0
+    assert np.array_equal(fl == wall, want)
+
+
+def test_stl_errors(tmp_path):
+    """An ASCII STL file and a bad side are errors with a message."""
+    lib = load_library()
+    lib.tclb_case_last_error.restype = ctypes.c_char_p
+    f = tmp_path / "ascii.stl"
+    write_stl_box(f, (1, 1, 1), (2, 2, 2), header=b"solid box")
+    dims = (ctypes.c_int * 3)()
+    out = np.zeros(32 * 8 * 8, np.uint16)
+    for elem, msg in ((f'<STL file="{f}"/>', b"binary"), (f'<STL file="{f}" side="top"/>', b"side")):
+        xml = f'<CLBConfig><Geometry nx="32" ny="8" nz="8"><Wall>{elem}</Wall></Geometry></CLBConfig>'
+        rc = lib.tclb_case_geometry(xml.encode(), M.get("d3q19").mid, dims,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), out.size)
+        assert rc != 0 and msg in lib.tclb_case_last_error()
+
+
+def test_sweep():
+    """<Sweep>: balls of radius 2.5 moved along the straight segment from x = 5 to
+    x = 25 at y = z = 8.5, as a linear B-spline of two points and as a quadratic
+    one of three collinear points. The balls lie at most ~0.26 apart, so every
+    node of the capsule around the segment is drawn and no other."""
+    wall = M.get("d3q19").flag("Wall")
+    z, y, x = np.meshgrid(np.arange(16), np.arange(16), np.arange(32), indexing="ij")
+    nearest = np.clip(0.5 + x, 5, 25)
+    want = (0.5 + x - nearest) ** 2 + (0.5 + y - 8.5) ** 2 + (0.5 + z - 8.5) ** 2 < 2.5 ** 2
+    for points in (((5, 8.5, 8.5), (25, 8.5, 8.5)), ((5, 8.5, 8.5), (12, 8.5, 8.5), (25, 8.5, 8.5))):
+        pts = "".join(f'<Point x="{a}" y="{b}" z="{c}"/>' for a, b, c in points)
+        fl = case_geometry(f'<CLBConfig><Geometry nx="32" ny="16" nz="16"><Wall><Sweep order="{len(points) - 1}" '
+                           f'r="2.5" step="0.001">{pts}</Sweep></Wall></Geometry></CLBConfig>', "d3q19")
+        assert np.array_equal(fl == wall, want), len(points)
+
+
 def test_bad_case_is_an_error_not_an_exit():
     lib = load_library()
     lib.tclb_case_last_error.restype = ctypes.c_char_p
