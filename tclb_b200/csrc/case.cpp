@@ -829,6 +829,13 @@ struct Callback {
   std::vector<int> stop_global, stop_kind;
   std::vector<double> stop_limit, stop_old;
   int stop_times = 1, stop_score = 0;
+  // <Sample> (src/Handlers/cbSample.cpp, src/Sampler.cpp): the sampled nodes,
+  // quantities, and the rows (values at every point) recorded since the last
+  // write, the first one labelled sample_start
+  std::vector<std::array<int, 3>> sample_pts;
+  std::vector<int> sample_q;
+  std::vector<double> sample_rows;
+  long long sample_start = 0;
   bool now(double it) const {  // vHandler::Now
     if (every <= 0) return false;
     it -= start;
@@ -1186,6 +1193,104 @@ struct Runner {
     if (data.size() != tclb_pri_bytes(lat)) throw CaseError(fn + " does not match this lattice");
     ck(tclb_load_pri(lat, data.data(), data.size()), "load .pri");
   }
+  // cbSample::Init (src/Handlers/cbSample.cpp:5-47), Sampler::initCSV
+  // (src/Sampler.cpp:16-36): the <Point dx dy dz> nodes inside the lattice
+  // (coordinates truncated to int), the `what` quantities (default all), and
+  // <case>_Sampler_P00_<iteration>.csv with the header
+  // Iteration,X,Y,Z,<quantity>[.x,.y,.z]...
+  void sample_init(Callback& c) {
+    if (c.every <= 0) throw CaseError("<Sample> needs Iterations > 0");
+    std::vector<std::string> what;
+    bool all = false;
+    {
+      std::stringstream ss(c.node->attr_or("what", "all"));
+      std::string w;
+      while (std::getline(ss, w, ','))
+        if (w == "all") all = true;
+        else what.push_back(w);
+    }
+    int nx, ny, nz;
+    tclb_get_size(lat, &nx, &ny, &nz);
+    for (const auto& ch : c.node->children) {
+      if (ch->name != "Point") throw CaseError("unknown element <" + ch->name + "> in <Sample>");
+      int p[3] = {0, 0, 0};
+      const char* k[3] = {"dx", "dy", "dz"};
+      for (int a = 0; a < 3; a++)
+        if (const std::string* v = ch->attr(k[a])) p[a] = (int)parse_value(*v);
+      if (p[0] >= 0 && p[1] >= 0 && p[2] >= 0 && p[0] < nx && p[1] < ny && p[2] < nz)
+        c.sample_pts.push_back({p[0], p[1], p[2]});
+    }
+    c.file = iter_file("Sampler", ".csv");
+    FILE* f = std::fopen(c.file.c_str(), "wt");
+    if (!f) throw CaseError("cannot write " + c.file);
+    std::fprintf(f, "Iteration,X,Y,Z");
+    for (int q = 0; q < T->nquantities; q++) {
+      const std::string qn = T->quantity_names[q];
+      if (!all && std::find(what.begin(), what.end(), qn) == what.end()) continue;
+      c.sample_q.push_back(q);
+      if (T->quantity_vector[q]) std::fprintf(f, ",%s.x,%s.y,%s.z", qn.c_str(), qn.c_str(), qn.c_str());
+      else std::fprintf(f, ",%s", qn.c_str());
+    }
+    std::fprintf(f, "\n");
+    std::fclose(f);
+    c.sample_start = iter;
+  }
+  // Lattice::updateAllSamples (src/Lattice.cu.Rt:1376-1390), after every
+  // iteration: the quantities at the sampled nodes, in SI units
+  void sample_record(Callback& c) {
+    const bool dbl = precision == TCLB_FP64;
+    for (const auto& p : c.sample_pts)
+      for (int q : c.sample_q) {
+        const int region[6] = {p[0], p[1], p[2], 1, 1, 1};
+        char buf[24];
+        ck(tclb_get_quantity(lat, q, region, buf, si_scale(model, T->quantity_names[q]), nullptr), "quantity");
+        for (int k = 0; k < (T->quantity_vector[q] ? 3 : 1); k++)
+          c.sample_rows.push_back(dbl ? reinterpret_cast<const double*>(buf)[k]
+                                      : (double)reinterpret_cast<const float*>(buf)[k]);
+      }
+  }
+  // cbSample::DoIt, Sampler::writeHistory (src/Sampler.cpp:37-62): one line per
+  // iteration since the last write and sampled node: the iteration, the node's
+  // X,Y,Z and its values (%g). TCLB prints only the x value of a vector
+  // quantity (it copies the three into one real_t); all three are written here,
+  // as its header names them.
+  void sample_write(Callback& c) {
+    FILE* f = std::fopen(c.file.c_str(), "at");
+    if (!f) throw CaseError("cannot write " + c.file);
+    size_t per_pt = 0;
+    for (int q : c.sample_q) per_pt += T->quantity_vector[q] ? 3 : 1;
+    const size_t per_row = per_pt * c.sample_pts.size();
+    const size_t rows = per_row ? c.sample_rows.size() / per_row : 0;
+    for (size_t r = 0; r < rows; r++)
+      for (size_t j = 0; j < c.sample_pts.size(); j++) {
+        std::fprintf(f, "%lld,%g,%g,%g", c.sample_start + (long long)r, (double)c.sample_pts[j][0],
+                     (double)c.sample_pts[j][1], (double)c.sample_pts[j][2]);
+        for (size_t k = 0; k < per_pt; k++) std::fprintf(f, ",%g", c.sample_rows[r * per_row + j * per_pt + k]);
+        std::fprintf(f, "\n");
+      }
+    std::fclose(f);
+    c.sample_rows.clear();
+    c.sample_start = iter;
+  }
+  // <SaveBinary> (src/Handlers/cbSaveBinary.cpp:5-33, Lattice::saveSolution
+  // src/Lattice.cu.Rt:240-249): the .pri snapshot to <name>_0.pri, the name
+  // fixed when the element is read. comp= saves only "parameter" densities
+  // (design variables of adjoint runs, Solver::saveComp), which the plain
+  // models do not have, so nothing is written, as in TCLB.
+  void save_binary(const Callback& c) {
+    if (const std::string* comp = c.node->attr("comp")) {
+      if (verbose) std::printf("[tclb_run] SaveBinary: no component %s; not saved\n", comp->c_str());
+      return;
+    }
+    std::vector<char> buf(tclb_pri_bytes(lat));
+    ck(tclb_save_pri(lat, buf.data(), buf.size()), "save .pri");
+    const std::string pri = c.file + "_0.pri";
+    FILE* o = std::fopen(pri.c_str(), "wb");
+    if (!o) throw CaseError("cannot write " + pri);
+    const size_t w = std::fwrite(buf.data(), 1, buf.size(), o);
+    std::fclose(o);
+    if (w != buf.size()) throw CaseError("cannot write " + pri);
+  }
   // <SaveCheckpoint> (src/Handlers/cbSaveCheckpoint.cpp:37-104): .pri plus a
   // restart case that loads it before <Solve>; keep = number retained.
   void save_checkpoint(const Callback& c) {
@@ -1292,6 +1397,12 @@ struct Runner {
       }
       iter_type |= TCLB_ITER_LASTGLOB;  // the Globals it checks
     }
+    if (c.kind == "Sample") sample_init(c);
+    if (c.kind == "SaveBinary") {  // cbSaveBinary::Init: the name is fixed here
+      if (const std::string* f = n->attr("file")) c.file = outpath + "_" + *f;
+      else if (const std::string* f = n->attr("filename")) c.file = *f;
+      else c.file = iter_file("Save", "");
+    }
     if (c.every > 0) {
       hands.push_back(c);
       return true;
@@ -1325,11 +1436,13 @@ struct Runner {
   // returns true to stop the solve
   bool do_callback(Callback& c) {
     if (c.kind == "Stop") return stop_check(c);
+    if (c.kind == "Sample") sample_write(c);
     if (c.kind == "VTK") write_vtk(c);
     if (c.kind == "TXT") write_txt(c);
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
+    else if (c.kind == "SaveBinary") save_binary(c);
     else if (c.kind == "Failcheck") {
       if (failcheck()) {
         std::printf("[tclb_run] Failcheck: non-finite values at iteration %lld, stopping\n", iter);
@@ -1358,9 +1471,15 @@ struct Runner {
         const int it = h.next((double)iter);
         if (it > 0 && it < next) next = it;
       }
+      bool sampling = false;  // <Sample> records every iteration
+      for (const auto& h : hands) sampling = sampling || h.kind == "Sample";
+      if (sampling) next = 1;
       int type = iter_type;
       if (next == my_next) type |= TCLB_ITER_LASTGLOB;
       ck(tclb_iterate(lat, next, type, nullptr), "iterate");
+      if (sampling)
+        for (auto& h : hands)
+          if (h.kind == "Sample") sample_record(h);
       iter += next;
       for (auto& h : hands)
         if (h.now((double)iter) && do_callback(h)) stop = true;
@@ -1385,7 +1504,8 @@ struct Runner {
       else if (n->name == "Init") init();
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
-               n->name == "Stop" || n->name == "VTK" || n->name == "TXT")
+               n->name == "Stop" || n->name == "VTK" || n->name == "TXT" || n->name == "SaveBinary" ||
+               n->name == "Sample")
         callback(n);
       else if (n->name == "LoadBinary") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)

@@ -426,6 +426,37 @@ def test_vtk_output(tmp_path):
 
 
 @pytest.mark.gpu
+def test_sample_output(tmp_path):
+    """<Sample>: after every iteration the chosen quantities at the <Point> nodes;
+    each Iterations period appends its rows to <case>_Sampler_P00_<it>.csv. The
+    row labelled 199 holds the state after the 200th iteration, the one the BIN
+    files hold."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    text = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    text = text.replace("<BIN ", '<Sample Iterations="50" what="Rho,U"><Point dx="100" dy="32"/>'
+                                 '<Point dx="30" dy="10"/><Point dx="900" dy="1"/></Sample><BIN ')
+    path = tmp_path / "case.xml"
+    path.write_text(text)
+    out = str(tmp_path / "out") + "/"
+    r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = open(out + "case_Sampler_P00_00000000.csv").read().strip().splitlines()
+    assert lines[0] == "Iteration,X,Y,Z,Rho,U.x,U.y,U.z"
+    rows = np.array([[float(v) for v in line.split(",")] for line in lines[1:]])
+    assert rows.shape == (200 * 2, 8)  # the point outside the lattice is dropped
+    assert np.array_equal(rows[::2, 0], np.arange(200)) and np.array_equal(rows[1::2, 0], np.arange(200))
+    assert np.all(rows[::2, 1:4] == [100, 32, 0]) and np.all(rows[1::2, 1:4] == [30, 10, 0])
+    rho = np.fromfile(out + "case_BIN_P00_00000200.Rho.bin", np.float32).reshape(64, 256)
+    u = np.fromfile(out + "case_BIN_P00_00000200.U.bin", np.float32).reshape(64, 256, 3)
+    for row, (x, y) in ((rows[-2], (100, 32)), (rows[-1], (30, 10))):
+        assert np.allclose(row[4], rho[y, x], rtol=1e-5, atol=0)
+        assert np.allclose(row[5:8], u[y, x], rtol=1e-5, atol=1e-12)
+    assert abs(rows[-2, 5] - rows[0, 5]) > 0  # the flow develops
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""

@@ -217,3 +217,26 @@ def test_checkpoint_restart_resumes_bit_exactly(tmp_path):
     assert pri.tobytes() == lat2.save_pri().tobytes()
     lat.close()
     lat2.close()
+
+
+@pytest.mark.gpu
+def test_save_binary(tmp_path):
+    """<SaveBinary>: the .pri snapshot to <out>_<file>_0.pri (the name fixed when
+    the element is read, so each call overwrites it), or without file= to
+    <out>_Save_P00_<iteration>_0.pri; both equal the checkpoint at the same
+    iteration. comp= names a parameter density, which these models lack, so
+    nothing is written."""
+    runner = os.path.join(ROOT, "tclb_b200", "tclb_run")
+    out = str(tmp_path) + "/"
+    text = CHECKPOINT_CASE.format(out=out).replace(
+        '<BIN Iterations="100"/>', '<SaveBinary Iterations="50" file="snap"/><SaveBinary Iterations="50" comp="Rho"/>')
+    text = text.replace("</Solve>", "</Solve>\n\t<SaveBinary/>")
+    case = tmp_path / "ck.xml"
+    case.write_text(text)
+    r = subprocess.run([runner, "d2q9", str(case), "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    ck = open(f"{out}ck_checkpoint_00000100_0.pri", "rb").read()
+    assert open(f"{out}ck_snap_0.pri", "rb").read() == ck
+    assert open(f"{out}ck_Save_P00_00000100_0.pri", "rb").read() == ck
+    assert open(f"{out}ck_checkpoint_00000050_0.pri", "rb").read() != ck
+    assert not [f for f in os.listdir(tmp_path) if "Rho" in f]
