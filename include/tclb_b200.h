@@ -198,8 +198,10 @@ int tclb_get_launch(tclb_h h, int* bx, int* by, int* flags);
 /* ---------------------------------------------------------------------------
    XML case files (<CLBConfig>): the control flow of TCLB's main and handler
    tree for the Run path (src/main.cpp:173-425, src/Handlers/acGeometry.cpp,
-   acModel.cpp, acParam.cpp, acInit.cpp, acSolve.cpp, cbLog.cpp, cbBIN.cpp,
-   cbFailcheck.cpp, cbStop.cpp, cbVTK.cpp, cbTXT.cpp, cbSaveBinary.cpp, cbSample.cpp). Values may carry units ("1e-6m2/s", "5mm+1cm");
+   acModel.cpp, acParam.cpp, acInit.cpp, acSolve.cpp, acContainer.cpp,
+   acRepeat.cpp, cbLog.cpp, cbBIN.cpp, cbFailcheck.cpp, cbStop.cpp, cbVTK.cpp,
+   cbTXT.cpp, cbSaveBinary.cpp, cbSample.cpp, cbAveraging.cpp). Values may carry
+   units ("1e-6m2/s", "5mm+1cm");
    <Units><Param value= gauge=> elements fix the lattice scale of each base
    unit as src/unit.cpp does, and the Log's _si columns use those scales.
    Unknown unit symbols are errors here (TCLB reads them as 0).

@@ -1491,9 +1491,23 @@ struct Runner {
   }
 
   void run(const XmlNode* cfg) {
-    for (const auto& cp : cfg->children) {
-      const XmlNode* n = cp.get();
-      if (n->name == "Geometry") geometry(n);
+    for (const auto& cp : cfg->children) element(cp.get());
+  }
+  // one element of <CLBConfig> or of a <Container> / <Repeat> (the handler
+  // factory's dispatch, src/HandlerFactory.h, src/Handlers/GenericAction.cpp)
+  void element(const XmlNode* n) {
+    {
+      if (n->name == "Container") {  // acContainer: the children, then unstack
+        const size_t stacked = hands.size();
+        for (const auto& c : n->children) element(c.get());
+        hands.resize(stacked);
+      } else if (n->name == "Repeat") {  // acRepeat: the children Times times; no unstack
+        const std::string* t = n->attr("Times");
+        if (!t) throw CaseError("<Repeat> needs Times");
+        const int times = std::atoi(t->c_str());
+        for (int i = 0; i < times; i++)
+          for (const auto& c : n->children) element(c.get());
+      } else if (n->name == "Geometry") geometry(n);
       else if (n->name == "Model") {  // acModel: params, then Init
         for (const auto& c : n->children) {
           if (c->name == "Param") param(c.get());

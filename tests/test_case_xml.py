@@ -457,6 +457,37 @@ def test_sample_output(tmp_path):
 
 
 @pytest.mark.gpu
+def test_repeat_and_container(tmp_path):
+    """<Repeat Times> runs its children that many times; <Container> runs its
+    children and then drops the callbacks they registered. Four 50-iteration
+    Solves in a Repeat and one more after the Container reach the state of one
+    250-iteration Solve bit for bit; the Log inside the Container stops with it."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    base = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    start = base.index("<Log ")
+    end = base.index("</CLBConfig>")
+    plain = base[:start] + '<Solve Iterations="250"/><BIN/>' + base[end:]
+    nested = (base[:start] + '<Container><Log Iterations="50"/><Repeat Times="4"><Solve Iterations="50"/>'
+              '</Repeat></Container><Solve Iterations="50"/><BIN/>' + base[end:])
+    outs = []
+    for name, text in (("plain", plain), ("nested", nested)):
+        path = tmp_path / f"{name}.xml"
+        path.write_text(text)
+        out = str(tmp_path / name) + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        outs.append(out)
+    for q in ("Rho", "U"):
+        a = open(outs[0] + f"plain_BIN_P00_00000250.{q}.bin", "rb").read()
+        b = open(outs[1] + f"nested_BIN_P00_00000250.{q}.bin", "rb").read()
+        assert a == b, q
+    log = open(outs[1] + "nested_Log_P00_00000000.csv").read().strip().splitlines()
+    assert [int(float(line.split(",")[0])) for line in log[1:]] == [50, 100, 150, 200]
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""
