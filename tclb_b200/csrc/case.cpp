@@ -1186,8 +1186,12 @@ struct Runner {
     need_lattice();
     const std::string* f = n->attr("file");
     if (!f) f = n->attr("filename");
-    if (!f) throw CaseError("<LoadBinary> needs a file attribute");
-    if (n->attr("comp")) throw CaseError("<LoadBinary comp=> (single fields) is not supported");
+    if (!f) throw CaseError("<" + n->name + "> needs a file attribute");
+    if (n->attr("comp")) {
+      // acLoadMemoryDump reports comp= as deprecated and loads the snapshot
+      if (n->name == "LoadBinary") throw CaseError("<LoadBinary comp=> (single fields) is not supported");
+      std::fprintf(stderr, "[tclb_run] <LoadMemoryDump comp=> is deprecated; loading the whole snapshot\n");
+    }
     const std::string fn = *f + "_0.pri";
     const std::string data = read_file(fn);
     if (data.size() != tclb_pri_bytes(lat)) throw CaseError(fn + " does not match this lattice");
@@ -1277,8 +1281,12 @@ struct Runner {
   // fixed when the element is read. comp= saves only "parameter" densities
   // (design variables of adjoint runs, Solver::saveComp), which the plain
   // models do not have, so nothing is written, as in TCLB.
+  // <SaveMemoryDump> (cbSaveMemoryDump.cpp) is the same without comp=: TCLB
+  // reports comp= there as deprecated and saves the snapshot.
   void save_binary(const Callback& c) {
-    if (const std::string* comp = c.node->attr("comp")) {
+    if (c.kind == "SaveMemoryDump" && c.node->attr("comp"))
+      std::fprintf(stderr, "[tclb_run] <SaveMemoryDump comp=> is deprecated; saving the whole snapshot\n");
+    else if (const std::string* comp = c.node->attr("comp")) {
       if (verbose) std::printf("[tclb_run] SaveBinary: no component %s; not saved\n", comp->c_str());
       return;
     }
@@ -1398,7 +1406,7 @@ struct Runner {
       iter_type |= TCLB_ITER_LASTGLOB;  // the Globals it checks
     }
     if (c.kind == "Sample") sample_init(c);
-    if (c.kind == "SaveBinary") {  // cbSaveBinary::Init: the name is fixed here
+    if (c.kind == "SaveBinary" || c.kind == "SaveMemoryDump") {  // cbSaveBinary::Init: the name is fixed here
       if (const std::string* f = n->attr("file")) c.file = outpath + "_" + *f;
       else if (const std::string* f = n->attr("filename")) c.file = *f;
       else c.file = iter_file("Save", "");
@@ -1442,7 +1450,7 @@ struct Runner {
     if (c.kind == "Log") log_row(c.file);
     else if (c.kind == "BIN") write_bin(iter_file(c.node->attr_or("name", "BIN"), ""));
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
-    else if (c.kind == "SaveBinary") save_binary(c);
+    else if (c.kind == "SaveBinary" || c.kind == "SaveMemoryDump") save_binary(c);
     else if (c.kind == "Failcheck") {
       if (failcheck()) {
         std::printf("[tclb_run] Failcheck: non-finite values at iteration %lld, stopping\n", iter);
@@ -1519,9 +1527,9 @@ struct Runner {
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
                n->name == "Stop" || n->name == "VTK" || n->name == "TXT" || n->name == "SaveBinary" ||
-               n->name == "Sample")
+               n->name == "Sample" || n->name == "SaveMemoryDump")
         callback(n);
-      else if (n->name == "LoadBinary") load_binary(n);
+      else if (n->name == "LoadBinary" || n->name == "LoadMemoryDump") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)
       } else if (n->name == "Average") {
         // cbAveraging (src/Handlers/cbAveraging.cpp:5-16) zeroes the densities a

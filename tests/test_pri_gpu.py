@@ -230,7 +230,7 @@ def test_save_binary(tmp_path):
     out = str(tmp_path) + "/"
     text = CHECKPOINT_CASE.format(out=out).replace(
         '<BIN Iterations="100"/>', '<SaveBinary Iterations="50" file="snap"/><SaveBinary Iterations="50" comp="Rho"/>')
-    text = text.replace("</Solve>", "</Solve>\n\t<SaveBinary/>")
+    text = text.replace("</Solve>", "</Solve>\n\t<SaveBinary/><SaveMemoryDump file=\"dump\"/>")
     case = tmp_path / "ck.xml"
     case.write_text(text)
     r = subprocess.run([runner, "d2q9", str(case), "--quiet"], capture_output=True, text=True)
@@ -240,3 +240,13 @@ def test_save_binary(tmp_path):
     assert open(f"{out}ck_Save_P00_00000100_0.pri", "rb").read() == ck
     assert open(f"{out}ck_checkpoint_00000050_0.pri", "rb").read() != ck
     assert not [f for f in os.listdir(tmp_path) if "Rho" in f]
+    assert open(f"{out}ck_dump_0.pri", "rb").read() == ck
+    # <LoadMemoryDump> reads it back: saved again right away, the bytes are the same
+    load = CHECKPOINT_CASE.format(out=out + "re_")
+    start, end = load.index("<Solve"), load.index("</CLBConfig>")
+    load = load[:start] + f'<LoadMemoryDump file="{out}ck_dump"/><SaveBinary file="again"/>\n' + load[end:]
+    case2 = tmp_path / "re.xml"
+    case2.write_text(load)
+    r = subprocess.run([runner, "d2q9", str(case2), "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert open(f"{out}re_re_again_0.pri", "rb").read() == ck
