@@ -1515,6 +1515,25 @@ struct Runner {
         const int times = std::atoi(t->c_str());
         for (int i = 0; i < times; i++)
           for (const auto& c : n->children) element(c.get());
+      } else if (n->name == "EvalIf") {
+        // IfContainer (src/Handlers/IfContainer.cpp:5-39): the children when the
+        // model option is present (opt_present) or absent (opt_missing). The
+        // plain variants built here have every option of their model off
+        // (conf.mk OPT=). TCLB's opt_missing branch reads the option name from
+        // the absent opt_present attribute and always fails; here it does
+        // what its name says.
+        const std::string* pres = n->attr("opt_present");
+        const std::string* miss = n->attr("opt_missing");
+        if ((pres != nullptr) == (miss != nullptr))
+          throw CaseError("<EvalIf> needs one of opt_present and opt_missing");
+        const std::string opt = pres ? *pres : *miss;
+        static const std::vector<std::string> options[3] = {{"bc", "autosym"}, {}, {"AVG", "IB", "SMAG"}};
+        const auto& known = options[model];
+        if (std::find(known.begin(), known.end(), opt) == known.end())
+          throw CaseError("unknown option in <EvalIf>: " + opt);
+        const bool active = false;
+        if (active == (pres != nullptr))
+          for (const auto& c : n->children) element(c.get());
       } else if (n->name == "Geometry") geometry(n);
       else if (n->name == "Model") {  // acModel: params, then Init
         for (const auto& c : n->children) {

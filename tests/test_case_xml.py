@@ -459,8 +459,10 @@ def test_sample_output(tmp_path):
 @pytest.mark.gpu
 def test_repeat_and_container(tmp_path):
     """<Repeat Times> runs its children that many times; <Container> runs its
-    children and then drops the callbacks they registered. Four 50-iteration
-    Solves in a Repeat and one more after the Container reach the state of one
+    children and then drops the callbacks they registered; <EvalIf> runs its
+    children when a model option is present (opt_present) or absent
+    (opt_missing), and the plain d2q9 has autosym off. Four 50-iteration Solves
+    in a Repeat and one more in the opt_missing branch reach the state of one
     250-iteration Solve bit for bit; the Log inside the Container stops with it."""
     import subprocess
 
@@ -470,7 +472,8 @@ def test_repeat_and_container(tmp_path):
     end = base.index("</CLBConfig>")
     plain = base[:start] + '<Solve Iterations="250"/><BIN/>' + base[end:]
     nested = (base[:start] + '<Container><Log Iterations="50"/><Repeat Times="4"><Solve Iterations="50"/>'
-              '</Repeat></Container><Solve Iterations="50"/><BIN/>' + base[end:])
+              '</Repeat></Container><EvalIf opt_present="autosym"><Solve Iterations="1000"/></EvalIf>'
+              '<EvalIf opt_missing="autosym"><Solve Iterations="50"/></EvalIf><BIN/>' + base[end:])
     outs = []
     for name, text in (("plain", plain), ("nested", nested)):
         path = tmp_path / f"{name}.xml"
