@@ -832,6 +832,11 @@ struct Callback {
   // <Sample> (src/Handlers/cbSample.cpp, src/Sampler.cpp): the sampled nodes,
   // quantities, and the rows (values at every point) recorded since the last
   // write, the first one labelled sample_start
+  // <PID> (src/Handlers/cbPID.cpp): the Global it integrates, the zonal
+  // setting (and zone, -1 for all) it drives, its constants and state
+  int pid_global = -1, pid_setting = -1, pid_zone = -1;
+  double pid_target = 0, pid_itime = 1, pid_dtime = 1, pid_scale = 1, pid_sval = 0, pid_integral = 0,
+         pid_old_err = 0;
   std::vector<std::array<int, 3>> sample_pts;
   std::vector<int> sample_q;
   std::vector<double> sample_rows;
@@ -1197,6 +1202,51 @@ struct Runner {
     if (data.size() != tclb_pri_bytes(lat)) throw CaseError(fn + " does not match this lattice");
     ck(tclb_load_pri(lat, data.data(), data.size()), "load .pri");
   }
+  // cbPID::Init (src/Handlers/cbPID.cpp:4-92): integral= names the Global,
+  // target= its goal, control= the zonal setting driven in zone= (all zones
+  // when absent); IntegrationTime, DerivativeTime and scale default to 1 s.
+  // The setting's value at this point (zone 0 for all zones) is the base the
+  // control is added to.
+  void pid_init(Callback& c) {
+    const XmlNode* n = c.node;
+    const std::string glob = n->attr_or("integral", "");
+    const std::string* target = n->attr("target");
+    if (!target) throw CaseError("<PID> needs a target");
+    c.pid_target = parse_value(*target);
+    if (glob.empty()) throw CaseError("<PID> needs integral= (a Global)");
+    for (int g = 0; g < T->nglobals; g++)
+      if (glob == T->global_names[g]) c.pid_global = g;
+    if (c.pid_global < 0) throw CaseError("unknown Global in <PID>: " + glob);
+    const std::string zone = n->attr_or("zone", "");
+    if (!zone.empty()) {
+      auto it = geo->zones.find(zone);
+      if (it == geo->zones.end()) throw CaseError("unknown zone in <PID>: " + zone);
+      c.pid_zone = it->second;
+    }
+    const std::string par = n->attr_or("control", "");
+    if (par.empty()) throw CaseError("<PID> needs control= (a zonal setting)");
+    c.pid_setting = zone_setting_index(par);
+    if (c.pid_setting < 0) throw CaseError(par + " is not a zonal setting (in <PID>)");
+    const double second = g_units.alt("1s");
+    c.pid_itime = n->attr("IntegrationTime") ? parse_value(*n->attr("IntegrationTime")) : second;
+    c.pid_dtime = n->attr("DerivativeTime") ? parse_value(*n->attr("DerivativeTime")) : second;
+    c.pid_scale = n->attr("scale") ? parse_value(*n->attr("scale")) : second;
+    ck(tclb_get_zone_setting(lat, c.pid_setting, c.pid_zone < 0 ? 0 : c.pid_zone, &c.pid_sval), "zone setting");
+    iter_type |= TCLB_ITER_LASTGLOB;
+  }
+  // cbPID::DoIt (:93-125): error = target - Global; trapezoid integral over
+  // the callback period DT; control = error + integral / IntegrationTime +
+  // derivative * DerivativeTime; setting = base + control * scale
+  void pid_step(Callback& c) {
+    std::vector<double> g(T->nglobals);
+    tclb_get_globals(lat, g.data());
+    const double dt = c.every, err = c.pid_target - g[c.pid_global];
+    c.pid_integral += (c.pid_old_err + err) * dt / 2.0;
+    const double derivative = (err - c.pid_old_err) / dt;
+    const double control = err + c.pid_integral / c.pid_itime + derivative * c.pid_dtime;
+    c.pid_old_err = err;
+    ck(tclb_set_zone_setting(lat, c.pid_setting, c.pid_zone, c.pid_sval + control * c.pid_scale), "zone setting");
+  }
   // cbSample::Init (src/Handlers/cbSample.cpp:5-47), Sampler::initCSV
   // (src/Sampler.cpp:16-36): the <Point dx dy dz> nodes inside the lattice
   // (coordinates truncated to int), the `what` quantities (default all), and
@@ -1406,6 +1456,7 @@ struct Runner {
       iter_type |= TCLB_ITER_LASTGLOB;  // the Globals it checks
     }
     if (c.kind == "Sample") sample_init(c);
+    if (c.kind == "PID") pid_init(c);
     if (c.kind == "SaveBinary" || c.kind == "SaveMemoryDump") {  // cbSaveBinary::Init: the name is fixed here
       if (const std::string* f = n->attr("file")) c.file = outpath + "_" + *f;
       else if (const std::string* f = n->attr("filename")) c.file = *f;
@@ -1445,6 +1496,7 @@ struct Runner {
   bool do_callback(Callback& c) {
     if (c.kind == "Stop") return stop_check(c);
     if (c.kind == "Sample") sample_write(c);
+    if (c.kind == "PID") pid_step(c);
     if (c.kind == "VTK") write_vtk(c);
     if (c.kind == "TXT") write_txt(c);
     if (c.kind == "Log") log_row(c.file);
@@ -1546,7 +1598,7 @@ struct Runner {
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
                n->name == "Stop" || n->name == "VTK" || n->name == "TXT" || n->name == "SaveBinary" ||
-               n->name == "Sample" || n->name == "SaveMemoryDump")
+               n->name == "Sample" || n->name == "SaveMemoryDump" || n->name == "PID")
         callback(n);
       else if (n->name == "LoadBinary" || n->name == "LoadMemoryDump") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)

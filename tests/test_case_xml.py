@@ -491,6 +491,43 @@ def test_repeat_and_container(tmp_path):
 
 
 @pytest.mark.gpu
+def test_pid_control(tmp_path):
+    """<PID>: every 10 iterations the inlet velocity becomes
+    base + scale * (e + integral / IntegrationTime + de/dt * DerivativeTime),
+    e = target - InletFlux, the integral by the trapezoid rule. The Log (checked
+    first, at the same iterations) holds each InletFlux and the velocity set at
+    the check before, so the whole control sequence is replayed from it."""
+    import csv
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    text = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    start, end = text.index("<Log "), text.index("</CLBConfig>")
+    text = (text[:start] + '<Solve Iterations="200"><Log Iterations="10"/><PID Iterations="10" integral="InletFlux" '
+            'target="1.0" control="VelocityX" zone="Inlet" IntegrationTime="200" DerivativeTime="2" '
+            'scale="2e-4"/></Solve>' + text[end:])
+    path = tmp_path / "case.xml"
+    path.write_text(text)
+    out = str(tmp_path / "out") + "/"
+    r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    with open(out + "case_Log_P00_00000000.csv") as f:
+        rows = list(csv.reader(f, skipinitialspace=True))
+    head = rows[0]
+    flux = np.array([float(r_[head.index("InletFlux")]) for r_ in rows[1:]])
+    vel = np.array([float(r_[head.index("VelocityX-Inlet")]) for r_ in rows[1:]])
+    assert len(flux) == 20 and vel[0] == 0.01
+    integral, old = 0.0, 0.0
+    for k in range(19):
+        err = 1.0 - flux[k]
+        integral += (old + err) * 10 / 2
+        control = err + integral / 200 + (err - old) / 10 * 2
+        old = err
+        assert vel[k + 1] == pytest.approx(0.01 + control * 2e-4, rel=1e-9, abs=1e-15), k
+    assert vel[-1] != vel[0]
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""
