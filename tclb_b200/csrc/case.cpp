@@ -837,6 +837,10 @@ struct Callback {
   int pid_global = -1, pid_setting = -1, pid_zone = -1;
   double pid_target = 0, pid_itime = 1, pid_dtime = 1, pid_scale = 1, pid_sval = 0, pid_integral = 0,
          pid_old_err = 0;
+  // <Keep> (src/Handlers/cbKeep.cpp): the Global, its InObj zonal setting,
+  // the threshold, the kind (1 Above, -1 Below, 0 Equal) and the force
+  int keep_global = -1, keep_inobj = -1, keep_type = 0;
+  double keep_thr = 0, keep_force = 1;
   std::vector<std::array<int, 3>> sample_pts;
   std::vector<int> sample_q;
   std::vector<double> sample_rows;
@@ -1202,6 +1206,37 @@ struct Runner {
     if (data.size() != tclb_pri_bytes(lat)) throw CaseError(fn + " does not match this lattice");
     ck(tclb_load_pri(lat, data.data(), data.size()), "load .pri");
   }
+  // cbKeep::Init (src/Handlers/cbKeep.cpp:5-43): What= names the Global; one
+  // of Above, Below or Equal gives the threshold; Force (default 1) the gain
+  void keep_init(Callback& c) {
+    const XmlNode* n = c.node;
+    const std::string* what = n->attr("What");
+    if (!what) throw CaseError("<Keep> needs What= (a Global)");
+    for (int g = 0; g < T->nglobals; g++)
+      if (*what == T->global_names[g]) c.keep_global = g;
+    if (c.keep_global < 0) throw CaseError("unknown Global in <Keep>: " + *what);
+    c.keep_inobj = zone_setting_index(*what + "InObj");
+    if (c.keep_inobj < 0) throw CaseError("<Keep>: " + *what + " has no InObj setting");
+    const std::string* thr;
+    if ((thr = n->attr("Above"))) c.keep_type = 1;
+    else if ((thr = n->attr("Below"))) c.keep_type = -1;
+    else if ((thr = n->attr("Equal"))) c.keep_type = 0;
+    else throw CaseError("<Keep> needs Above, Below or Equal");
+    c.keep_thr = std::atof(thr->c_str());
+    if (const std::string* f = n->attr("Force")) c.keep_force = std::atof(f->c_str());
+    iter_type |= TCLB_ITER_LASTGLOB;
+  }
+  // cbKeep::DoIt (:46-66): v = (threshold - Global) * Force; the Global's InObj
+  // weight in every zone becomes v when it points the kept way (v > 0 for
+  // Above, v < 0 for Below, always for Equal), else 0
+  void keep_step(Callback& c) {
+    std::vector<double> g(T->nglobals);
+    tclb_get_globals(lat, g.data());
+    const double v = (c.keep_thr - g[c.keep_global]) * c.keep_force;
+    double s = 0.0;
+    if (c.keep_type == 0 || (c.keep_type == 1 && v > 0) || (c.keep_type == -1 && v < 0)) s = v;
+    ck(tclb_set_zone_setting(lat, c.keep_inobj, -1, s), "zone setting");
+  }
   // cbPID::Init (src/Handlers/cbPID.cpp:4-92): integral= names the Global,
   // target= its goal, control= the zonal setting driven in zone= (all zones
   // when absent); IntegrationTime, DerivativeTime and scale default to 1 s.
@@ -1457,6 +1492,7 @@ struct Runner {
     }
     if (c.kind == "Sample") sample_init(c);
     if (c.kind == "PID") pid_init(c);
+    if (c.kind == "Keep") keep_init(c);
     if (c.kind == "SaveBinary" || c.kind == "SaveMemoryDump") {  // cbSaveBinary::Init: the name is fixed here
       if (const std::string* f = n->attr("file")) c.file = outpath + "_" + *f;
       else if (const std::string* f = n->attr("filename")) c.file = *f;
@@ -1497,6 +1533,7 @@ struct Runner {
     if (c.kind == "Stop") return stop_check(c);
     if (c.kind == "Sample") sample_write(c);
     if (c.kind == "PID") pid_step(c);
+    if (c.kind == "Keep") keep_step(c);
     if (c.kind == "VTK") write_vtk(c);
     if (c.kind == "TXT") write_txt(c);
     if (c.kind == "Log") log_row(c.file);
@@ -1598,7 +1635,8 @@ struct Runner {
       else if (n->name == "Solve") solve(n);
       else if (n->name == "Log" || n->name == "BIN" || n->name == "Failcheck" || n->name == "SaveCheckpoint" ||
                n->name == "Stop" || n->name == "VTK" || n->name == "TXT" || n->name == "SaveBinary" ||
-               n->name == "Sample" || n->name == "SaveMemoryDump" || n->name == "PID")
+               n->name == "Sample" || n->name == "SaveMemoryDump" || n->name == "PID" ||
+               n->name == "Keep")
         callback(n);
       else if (n->name == "LoadBinary" || n->name == "LoadMemoryDump") load_binary(n);
       else if (n->name == "Units") {  // read before the run (read_units)

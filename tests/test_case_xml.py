@@ -528,6 +528,39 @@ def test_pid_control(tmp_path):
 
 
 @pytest.mark.gpu
+def test_keep(tmp_path):
+    """<Keep What="InletFlux" Above=...>: at each check InletFluxInObj becomes
+    (threshold - InletFlux) * Force in every zone when that is positive, else 0;
+    the Log (checked first) shows the value set at the check before."""
+    import csv
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    text = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    start, end = text.index("<Log "), text.index("</CLBConfig>")
+    outs = {}
+    for kind, thr in (("Above", "0.7"), ("Below", "0.7"), ("Equal", "0.5")):
+        case = (text[:start] + f'<Solve Iterations="100"><Log Iterations="10"/><Keep Iterations="10" What="InletFlux" '
+                f'{kind}="{thr}" Force="3"/></Solve>' + text[end:])
+        path = tmp_path / f"{kind}.xml"
+        path.write_text(case)
+        out = str(tmp_path / kind) + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        with open(out + f"{kind}_Log_P00_00000000.csv") as f:
+            rows = list(csv.reader(f, skipinitialspace=True))
+        head = rows[0]
+        flux = np.array([float(r_[head.index("InletFlux")]) for r_ in rows[1:]])
+        for zone in ("Inlet", "Outlet"):
+            w = np.array([float(r_[head.index(f"InletFluxInObj-{zone}")]) for r_ in rows[1:]])
+            v = (float(thr) - flux[:-1]) * 3
+            want = {"Above": np.where(v > 0, v, 0), "Below": np.where(v < 0, v, 0), "Equal": v}[kind]
+            assert np.allclose(w[1:], want, rtol=1e-12, atol=1e-15), (kind, zone)
+        outs[kind] = flux
+    assert (outs["Equal"] != 0).all()
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""
