@@ -201,9 +201,8 @@ int tclb_get_launch(tclb_h h, int* bx, int* by, int* flags);
    acModel.cpp, acParam.cpp, acInit.cpp, acSolve.cpp, acContainer.cpp,
    acRepeat.cpp, cbLog.cpp, cbBIN.cpp, cbFailcheck.cpp, cbStop.cpp, cbVTK.cpp,
    cbTXT.cpp, cbSaveBinary.cpp, cbSample.cpp, cbPID.cpp, cbKeep.cpp,
-   cbAveraging.cpp,
-   IfContainer.cpp). Values may carry
-   units ("1e-6m2/s", "5mm+1cm");
+   cbAveraging.cpp, IfContainer.cpp). Values may carry units ("1e-6m2/s",
+   "5mm+1cm");
    <Units><Param value= gauge=> elements fix the lattice scale of each base
    unit as src/unit.cpp does, and the Log's _si columns use those scales.
    Unknown unit symbols are errors here (TCLB reads them as 0).
