@@ -1559,7 +1559,7 @@ struct Runner {
     if (self.every <= 0) throw CaseError("<Solve> needs Iterations > 0");
     const size_t stacked = hands.size();
     const int saved_type = iter_type;
-    for (const auto& c : n->children) callback(c.get());
+    for (const auto& c : n->children) element(c.get());  // ExecuteInternal: actions now, callbacks stacked
     bool stop = false;
     do {
       const int my_next = self.next((double)iter);

@@ -561,6 +561,31 @@ def test_keep(tmp_path):
 
 
 @pytest.mark.gpu
+def test_param_inside_solve(tmp_path):
+    """A <Param> among a <Solve>'s children takes effect when the Solve starts
+    (acSolve runs its children like any container): the same state as the Param
+    placed just before the Solve."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    base = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
+    start, end = base.index("<Log "), base.index("</CLBConfig>")
+    param = '<Param name="VelocityX" value="0.02" zone="Inlet"/>'
+    texts = {"before": base[:start] + param + '<Solve Iterations="100"><BIN Iterations="100"/></Solve>' + base[end:],
+             "inside": base[:start] + '<Solve Iterations="100">' + param + '<BIN Iterations="100"/></Solve>' + base[end:],
+             "none": base[:start] + '<Solve Iterations="100"><BIN Iterations="100"/></Solve>' + base[end:]}
+    u = {}
+    for name, text in texts.items():
+        path = tmp_path / f"{name}.xml"
+        path.write_text(text)
+        out = str(tmp_path / name) + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        u[name] = open(out + f"{name}_BIN_P00_00000100.U.bin", "rb").read()
+    assert u["inside"] == u["before"] and u["inside"] != u["none"]
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""
