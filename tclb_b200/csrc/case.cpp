@@ -1132,6 +1132,8 @@ struct Runner {
       std::vector<char> buf(size * comp * (dbl ? 8 : 4));
       ck(tclb_get_quantity(lat, q, nullptr, buf.data(), si_scale(model, qn), nullptr), "quantity");
       const std::string fn = base + "_" + qn + ".txt";
+      // the file name goes to the shell inside single quotes, so it may not hold one
+      if (gzip && fn.find('\'') != std::string::npos) throw CaseError("<TXT gzip>: quote in file name " + fn);
       FILE* f = gzip ? popen(("gzip > '" + fn + ".gz'").c_str(), "w") : std::fopen(fn.c_str(), "w");
       if (!f) throw CaseError("cannot write " + fn);
       for (size_t i = 0; i < size; i++) {
