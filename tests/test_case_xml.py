@@ -593,7 +593,7 @@ def test_txt_output(tmp_path):
 
     runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
     text = open(os.path.join(HERE, "cases", "channel_disc.xml")).read()
-    text = text.replace("<BIN ", '<TXT Iterations="200"/><BIN ')
+    text = text.replace("<BIN ", '<TXT Iterations="200"/><TXT Iterations="200" name="Z" what="Rho" gzip="true"/><BIN ')
     path = tmp_path / "case.xml"
     path.write_text(text)
     out = str(tmp_path / "out") + "/"
@@ -610,6 +610,11 @@ def test_txt_output(tmp_path):
     assert u.shape == (64, 256 * 3)
     u_bin = np.fromfile(out + "case_BIN_P00_00000200.U.bin", np.float32).reshape(64, 256 * 3)
     assert np.allclose(u, u_bin, rtol=1e-7, atol=1e-30)
+    import gzip
+    zbase = out + "case_Z_P00_00000200"
+    with gzip.open(zbase + "_Rho.txt.gz", "rt") as f:
+        assert np.array_equal(np.loadtxt(f), rho)
+    assert not os.path.exists(zbase + "_U.txt.gz")
 
 
 @pytest.mark.gpu
