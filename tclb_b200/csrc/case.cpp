@@ -841,6 +841,8 @@ struct Callback {
   // the threshold, the kind (1 Above, -1 Below, 0 Equal) and the force
   int keep_global = -1, keep_inobj = -1, keep_type = 0;
   double keep_thr = 0, keep_force = 1;
+  // <Failcheck>: the checked region (x0, y0, z0, nx, ny, nz)
+  int fc_region[6] = {0, 0, 0, 1, 1, 1};
   std::vector<std::array<int, 3>> sample_pts;
   std::vector<int> sample_q;
   std::vector<double> sample_rows;
@@ -1170,25 +1172,52 @@ struct Runner {
     }
   }
   // cbFailcheck: stop when a quantity is not finite
-  bool failcheck() {
-    int nx, ny, nz;
-    tclb_get_size(lat, &nx, &ny, &nz);
-    const size_t N = (size_t)nx * ny * nz;
-    for (int q = 0; q < T->nquantities; q++) {
+  // cbFailcheck (src/Handlers/cbFailcheck.cpp:4-88): the `what` quantities
+  // (default all) over the region dx..nz, which defaults to the one node at
+  // the origin (lbRegion's default size 1 x 1 x 1; TCLB's examples give nx, ny
+  // and nz), clipped to the lattice. NaN (not Inf) fails the check; the
+  // element's children then run as final actions before the stop. TCLB sets a
+  // re-entrancy flag at its first check and never clears it, so it checks
+  // once; here every call checks.
+  bool failcheck(const Callback& c) {
+    int dims[3];
+    tclb_get_size(lat, &dims[0], &dims[1], &dims[2]);
+    int reg[6];
+    for (int a = 0; a < 3; a++) {
+      const int lo = std::max(c.fc_region[a], 0), hi = std::min(c.fc_region[a] + c.fc_region[3 + a], dims[a]);
+      if (hi <= lo) return false;
+      reg[a] = lo, reg[3 + a] = hi - lo;
+    }
+    const size_t N = (size_t)reg[3] * reg[4] * reg[5];
+    std::vector<std::string> what;
+    bool all = false;
+    {
+      std::stringstream ss(c.node->attr_or("what", "all"));
+      std::string w;
+      while (std::getline(ss, w, ','))
+        if (w == "all") all = true;
+        else what.push_back(w);
+    }
+    bool nan = false;
+    for (int q = 0; q < T->nquantities && !nan; q++) {
+      if (!all && std::find(what.begin(), what.end(), T->quantity_names[q]) == what.end()) continue;
       const int comp = T->quantity_vector[q] ? 3 : 1;
       if (precision == TCLB_FP64) {
         std::vector<double> b(N * comp);
-        ck(tclb_get_quantity(lat, q, nullptr, b.data(), 1.0, nullptr), "quantity");
-        for (double v : b)
-          if (!std::isfinite(v)) return true;
+        ck(tclb_get_quantity(lat, q, reg, b.data(), 1.0, nullptr), "quantity");
+        for (double v : b) nan = nan || std::isnan(v);
       } else {
         std::vector<float> b(N * comp);
-        ck(tclb_get_quantity(lat, q, nullptr, b.data(), 1.0, nullptr), "quantity");
-        for (float v : b)
-          if (!std::isfinite(v)) return true;
+        ck(tclb_get_quantity(lat, q, reg, b.data(), 1.0, nullptr), "quantity");
+        for (float v : b) nan = nan || std::isnan(v);
       }
     }
-    return false;
+    if (!nan) return false;
+    for (const auto& ch : c.node->children) {  // final actions
+      Callback f = make_callback(ch.get());
+      do_callback(f);
+    }
+    return true;
   }
 
   // <LoadBinary file=> (src/Handlers/acLoadBinary.cpp): Lattice::loadSolution
@@ -1461,6 +1490,16 @@ struct Runner {
 
   // Handler of a callback element; returns true when it registered (has Iterations)
   bool callback(const XmlNode* n) {
+    Callback c = make_callback(n);
+    if (c.every > 0) {
+      hands.push_back(c);
+      return true;
+    }
+    do_callback(c);  // no Iterations: runs once, now (GenericAction::ExecuteInternal)
+    return false;
+  }
+  // the handler's Init: what it reads and prepares when the element is read
+  Callback make_callback(const XmlNode* n) {
     need_lattice();
     Callback c;
     c.kind = n->name;
@@ -1500,12 +1539,12 @@ struct Runner {
       else if (const std::string* f = n->attr("filename")) c.file = *f;
       else c.file = iter_file("Save", "");
     }
-    if (c.every > 0) {
-      hands.push_back(c);
-      return true;
+    if (c.kind == "Failcheck") {  // cbFailcheck::Init: the checked region
+      const char* k[6] = {"dx", "dy", "dz", "nx", "ny", "nz"};
+      for (int a = 0; a < 6; a++)
+        if (const std::string* v = n->attr(k[a])) c.fc_region[a] = (int)parse_value(*v);
     }
-    do_callback(c);  // no Iterations: runs once, now (GenericAction::ExecuteInternal)
-    return false;
+    return c;
   }
   // cbStop::DoIt: true when every criterion has held on Times consecutive checks
   bool stop_check(Callback& c) {
@@ -1543,8 +1582,8 @@ struct Runner {
     else if (c.kind == "SaveCheckpoint") save_checkpoint(c);
     else if (c.kind == "SaveBinary" || c.kind == "SaveMemoryDump") save_binary(c);
     else if (c.kind == "Failcheck") {
-      if (failcheck()) {
-        std::printf("[tclb_run] Failcheck: non-finite values at iteration %lld, stopping\n", iter);
+      if (failcheck(c)) {
+        std::printf("[tclb_run] Failcheck: NaN at iteration %lld, stopping\n", iter);
         return true;
       }
     }

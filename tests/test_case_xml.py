@@ -586,6 +586,40 @@ def test_param_inside_solve(tmp_path):
 
 
 @pytest.mark.gpu
+def test_failcheck_stops_and_runs_final_actions(tmp_path):
+    """<Failcheck> over the whole lattice (nx, ny given, as TCLB's examples do):
+    a negative viscosity makes the run overflow to NaN (plain IEEE arithmetic);
+    the check stops the Solve at its first failing call and runs its child
+    <VTK> there first. A Failcheck with a what= list naming no quantity checks
+    nothing and never stops the run."""
+    import subprocess
+
+    runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
+    base = open(os.path.join(HERE, "cases", "channel_disc.xml")).read().replace(
+        '<Param name="Viscosity" value="0.02"/>', '<Param name="Viscosity" value="-0.2"/>')
+    start, end = base.index("<Log "), base.index("</CLBConfig>")
+    for name, fc, stops in (("whole", '<Failcheck Iterations="10" nx="256" ny="64"><VTK what="Rho"/></Failcheck>', True),
+                            ("none", '<Failcheck Iterations="10" nx="256" ny="64" what="NoSuch"/>', False)):
+        text = base[:start] + f'<Solve Iterations="300">{fc}<BIN Iterations="300"/></Solve>' + base[end:]
+        path = tmp_path / f"{name}.xml"
+        path.write_text(text)
+        out = str(tmp_path / name) + "/"
+        r = subprocess.run([runner, "d2q9", str(path), "--output", out, "--quiet"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        files = os.listdir(out)
+        bins = [f for f in files if "_BIN_" in f]
+        vtis = [f for f in files if f.endswith(".vti")]
+        if stops:
+            assert not bins and len(vtis) == 1, files
+            it = int(vtis[0].split("_P00_")[1][:8])
+            assert it % 10 == 0 and 0 < it < 300
+            rho = read_vti(out + vtis[0])[0]["Rho"]
+            assert np.isnan(rho).any()
+        else:
+            assert bins and not vtis, files
+
+
+@pytest.mark.gpu
 def test_txt_output(tmp_path):
     """<TXT>: the info file and one text file per quantity (SI units; rows of
     nx nodes; vectors x y z per node), the same values as the BIN files."""
