@@ -802,6 +802,13 @@ struct Geometry {
           else throw CaseError("unknown mode " + a.second);
         }
       }
+      // zone="..." draws that <Zone> (the case's own or a default one) first
+      // (Geometry::loadZone :1127-1137); an unknown name is reported and skipped,
+      // as TCLB does
+      if (const std::string* z = n->attr("zone")) {
+        if (const XmlNode* zn = find_zone(*z)) draw(zn);
+        else std::fprintf(stderr, "[tclb_run] unknown zone %s in <%s>\n", z->c_str(), n->name.c_str());
+      }
       draw(n);
     }
   }

@@ -267,6 +267,22 @@ def test_sweep():
         assert np.array_equal(fl == wall, want), len(points)
 
 
+def test_zone_attribute_draws_the_zone():
+    """A flag element's zone= attribute draws that <Zone> (here one of the case's
+    own, and the default Inlet) before the element's own children."""
+    wall = M.get("d2q9").flag("Wall")
+    fl = case_geometry("""<CLBConfig><Geometry nx="32" ny="8">
+      <Zone name="blk"><Box dx="2" nx="3" dy="1" ny="2"/></Zone>
+      <Wall zone="blk"><Box dx="10" nx="1" dy="5" ny="1"/></Wall>
+      <Solid zone="Inlet"/>
+    </Geometry></CLBConfig>""", "d2q9")
+    want = np.zeros((1, 8, 32), np.uint16)
+    want[0, 1:3, 2:5] = wall
+    want[0, 5, 10] = wall
+    want[0, :, 0] = M.get("d2q9").flag("Solid")  # the default Inlet zone: the x = 0 column
+    assert np.array_equal(fl, want)
+
+
 def test_bad_case_is_an_error_not_an_exit():
     lib = load_library()
     lib.tclb_case_last_error.restype = ctypes.c_char_p
