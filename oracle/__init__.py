@@ -37,6 +37,7 @@ def lib():
         L.orc_create.argtypes = [i, i, i, i, i]
         L.orc_destroy.argtypes = [vp]
         L.orc_set_threads.argtypes = [i]
+        L.orc_set_storage.argtypes = [vp, i, ctypes.c_uint, d]
         L.orc_set_flags.argtypes = [vp, ctypes.POINTER(ctypes.c_uint16)]
         L.orc_set_setting.argtypes = [vp, i, d]
         L.orc_get_setting.argtypes = [vp, i, dp]
@@ -86,6 +87,15 @@ class OracleLattice:
         if h:
             lib().orc_destroy(h)
             self._h = None
+
+    STORAGE_EMULATION = {"same": 0, "fp16s": 1, "fp16s_sr": 2, "bf16s": 3, "bf16s_sr": 4, "mant": 5, "fixed": 6, "exm": 7}
+
+    def set_storage(self, storage: str, seed: int = 0, param: float = 0.0):
+        """Emulate a shifted storage format on every store (FP32 oracle): f is kept as
+        decode(encode(float(f - w_i))) + w_i. "_sr" rounds stochastically; "mant" keeps
+        `param` mantissa bits; "fixed" stores (f - w_i) as a 16-bit count of w_i * param / 32768."""
+        if lib().orc_set_storage(self._h, self.STORAGE_EMULATION[storage], seed, float(param)) != 0:
+            raise ValueError(storage)
 
     def set_flags(self, flags: np.ndarray):
         fl = np.ascontiguousarray(flags, dtype=np.uint16).reshape(-1)

@@ -485,6 +485,118 @@ struct Ops {
 // ---------------------------------------------------------------------------
 // Lattice
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Storage emulation: the checker for the CUDA library's 16-bit storage
+// formats. A population is stored as g = float(f - w_i) (TCLB's half-shift,
+// src/LatticeAccess.inc.cpp.Rt:29-35) rounded to the format, and read back as
+// decode(g) + w_i. The conversions are written here from the IEEE 754
+// binary16 and bfloat16 definitions with integer bit operations; "stochastic"
+// rounding rounds the magnitude up with probability equal to the discarded
+// fraction, using 32 random bits per value from the integer hash below.
+// ---------------------------------------------------------------------------
+enum StorageEmu { EMU_NONE = 0, EMU_F16_RN = 1, EMU_F16_SR = 2, EMU_BF16_RN = 3, EMU_BF16_SR = 4, EMU_MANT = 5,
+                  EMU_FIXED = 6, EMU_EXM = 7 };
+
+// 32-bit integer hash "lowbias32" (C. Wellons, "Prospecting for Hash Functions", 2018).
+static inline uint32_t hash32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+static inline uint32_t f2u(float v) { uint32_t b; std::memcpy(&b, &v, 4); return b; }
+static inline float u2f(uint32_t b) { float v; std::memcpy(&v, &b, 4); return v; }
+
+// float -> binary16 bits; sr: round up the magnitude when discarded + (rnd & mask) carries.
+static uint16_t f32_to_f16(float v, bool sr, uint32_t rnd) {
+  const uint32_t b = f2u(v), s = (b >> 16) & 0x8000u, a = b & 0x7fffffffu;
+  if (a >= 0x7f800000u) return (uint16_t)(s | 0x7c00u | (a > 0x7f800000u ? 0x200u : 0));
+  const int e = (int)(a >> 23) - 127;
+  if (e >= -14) {  // binary16 normal range: drop 13 mantissa bits
+    uint32_t val = ((uint32_t)(e + 15) << 10) | ((a & 0x7fffffu) >> 13);
+    const uint32_t rem = a & 0x1fffu;
+    if (sr) val += (rem + (rnd & 0x1fffu)) >> 13;
+    else if (rem > 0x1000u || (rem == 0x1000u && (val & 1u))) val++;
+    if (val >= 0x7c00u) val = 0x7c00u;  // overflow: infinity
+    return (uint16_t)(s | val);
+  }
+  // subnormal: units of 2^-24; the 24-bit significand times 2^(e+1)
+  const int shift = -e - 1;
+  if (shift > 31) return (uint16_t)s;
+  const uint64_t mf = (a & 0x7fffffu) | 0x800000u;
+  uint64_t q = mf >> shift;
+  const uint64_t rem = mf & ((1ull << shift) - 1), full = 1ull << shift;
+  if (sr) q += (rem + ((uint64_t)rnd & (full - 1))) >> shift;
+  else if (rem > full / 2 || (rem == full / 2 && (q & 1))) q++;
+  return (uint16_t)(s | (uint32_t)q);
+}
+static float f16_to_f32(uint16_t h) {
+  const uint32_t s = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1f, m = h & 0x3ffu;
+  if (e == 0x1f) return u2f(s | 0x7f800000u | (m << 13));
+  if (e == 0) return (s ? -1.0f : 1.0f) * (float)m * 5.9604644775390625e-8f;  // m * 2^-24
+  return u2f(s | ((e + 112) << 23) | (m << 13));
+}
+static uint16_t f32_to_bf16(float v, bool sr, uint32_t rnd) {
+  const uint32_t b = f2u(v);
+  if ((b & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((b >> 16) | 0x40u);
+  if (sr) return (uint16_t)((b + (rnd & 0xffffu)) >> 16);  // magnitude bits carry on sign-magnitude
+  return (uint16_t)((b + 0x7fffu + ((b >> 16) & 1u)) >> 16);
+}
+static float bf16_to_f32(uint16_t h) { return u2f((uint32_t)h << 16); }
+
+// Random bits of population i of node n written by iteration it.
+static inline uint32_t storage_bits(uint32_t seed, long it, size_t n, int i) {
+  return hash32(hash32((uint32_t)n ^ seed) + hash32((uint32_t)(it * 27 + i)));
+}
+
+// g rounded to nearest with k explicit mantissa bits (FP32 exponent range)
+static inline float round_mantissa(float g, int k) {
+  const uint32_t b = f2u(g), drop = 23 - k, half = 1u << (drop - 1), rem = b & ((1u << drop) - 1);
+  uint32_t r = b - rem;
+  if (rem > half || (rem == half && ((b >> drop) & 1u))) r += 1u << drop;
+  return u2f(r);
+}
+// g stored as a signed 16-bit integer count of w * scale / 32768
+static inline float round_fixed(float g, double w, double scale) {
+  const double unit = w * scale / 32768.0;
+  double q = std::nearbyint((double)g / unit);
+  q = std::min(32767.0, std::max(-32768.0, q));
+  return (float)(q * unit);
+}
+
+// h = g / w in a 16-bit float with E exponent bits, 15 - E mantissa bits and top S (param = E * 16 + log2(1/S)):
+// binades [S 2^-k-1, S 2^-k) for k < 2^E - 1, then a subnormal range of spacing S 2^-(2^E - 1) 2^-(15-E).
+static inline float round_exm(float g, double w, double param) {
+  const int E = (int)param / 16, L = (int)param % 16, M = 15 - E;
+  const double S = std::ldexp(1.0, -L), h = (double)g / w, a = std::fabs(h);
+  const int nb = (1 << E) - 1;  // normal binades
+  int k = 0;                    // binade below the top
+  double unit;
+  if (a >= S) return (float)(std::copysign(S - std::ldexp(S, -1 - M), h) * w);  // saturate (not reached here)
+  if (E == 0) unit = std::ldexp(S, -M);
+  else {
+    while (k < nb && a < std::ldexp(S, -1 - k)) k++;
+    unit = k < nb ? std::ldexp(S, -1 - k - M) : std::ldexp(S, -nb - M);
+  }
+  const double q = std::nearbyint(a / unit) * unit;
+  return (float)(std::copysign(std::min(q, S - std::ldexp(S, -1 - M)), h) * w);
+}
+
+template <class R>
+static inline R storage_roundtrip(int mode, R f, double w, uint32_t rnd, double param = 0) {
+  const float wf = (float)w, g = (float)f - wf;
+  float d;
+  switch (mode) {
+    case EMU_MANT: d = round_mantissa(g, (int)param); break;
+    case EMU_FIXED: d = round_fixed(g, w, param); break;
+    case EMU_EXM: d = round_exm(g, w, param); break;
+    case EMU_F16_RN: d = f16_to_f32(f32_to_f16(g, false, 0)); break;
+    case EMU_F16_SR: d = f16_to_f32(f32_to_f16(g, true, rnd)); break;
+    case EMU_BF16_RN: d = bf16_to_f32(f32_to_bf16(g, false, 0)); break;
+    case EMU_BF16_SR: d = bf16_to_f32(f32_to_bf16(g, true, rnd)); break;
+    default: return f;
+  }
+  return (R)(d + wf);
+}
+
 struct GlobAcc {
   std::vector<double> v;
 };
@@ -506,6 +618,10 @@ struct Lattice {
   std::vector<double> dev_globals;  // per-iteration integrated globals (device side in TCLB)
   std::vector<double> globals;      // host accumulators (Lattice::globals)
   long iter = 0;
+  int storage_mode = EMU_NONE;  // storage emulation of the iteration's stores
+  uint32_t storage_seed = 0;
+  double storage_param = 0;     // EMU_MANT: mantissa bits; EMU_FIXED: range of (f - w) / w
+  std::vector<double> wts;      // lattice weights: the storage shift
 
   Lattice(int m, int nx_, int ny_, int nz_) : model(m), nx(nx_), ny(ny_), nz(nz_) {
     ops.build(m);
@@ -524,6 +640,8 @@ struct Lattice {
       for (int s = 0; s < I.nzs; s++) zone[(size_t)z * I.nzs + s] = I.zs_default[s];
     dev_globals.assign(2 * I.nglob, 0.0);
     globals.assign(2 * I.nglob, 0.0);
+    wts.resize(Q);
+    for (int i = 0; i < Q; i++) wts[i] = ops.feq[i].a;  // feq at rho = 1, J = 0
   }
 
   void set_setting(int i, double v) {  // Lattice::SetSetting (src/Lattice.cu.Rt:1350-1358)
@@ -1044,6 +1162,12 @@ struct Lattice {
 
   void node_pull(const std::vector<R>& src, int x, int y, int z, R* f) const {
     const int* e = ops.L.e.data();
+    const size_t n = nidx(x, y, z);
+    if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {  // no wrap: a fixed offset
+      for (int i = 0; i < ops.L.Q; i++)
+        f[i] = src[(size_t)i * N + n - ((ptrdiff_t)e[i * 3] + (ptrdiff_t)nx * (e[i * 3 + 1] + (ptrdiff_t)ny * e[i * 3 + 2]))];
+      return;
+    }
     for (int i = 0; i < ops.L.Q; i++) {
       int xs = (x - e[i * 3] + nx) % nx, ys = (y - e[i * 3 + 1] + ny) % ny, zs = (z - e[i * 3 + 2] + nz) % nz;
       f[i] = src[(size_t)i * N + nidx(xs, ys, zs)];
@@ -1080,7 +1204,12 @@ struct Lattice {
           size_t n = nidx(x, y, z);
           node_pull(src, x, y, z, f);
           run_node(f, flags[n], G);
-          for (int i = 0; i < Q; i++) dst[(size_t)i * N + n] = f[i];
+          if (storage_mode)
+            for (int i = 0; i < Q; i++)
+              dst[(size_t)i * N + n] =
+                  storage_roundtrip(storage_mode, f[i], wts[i], storage_bits(storage_seed, iter, n, i), storage_param);
+          else
+            for (int i = 0; i < Q; i++) dst[(size_t)i * N + n] = f[i];
         }
       }
     if (glob) {
@@ -1264,6 +1393,14 @@ void orc_destroy(void* p) {
   delete h;
 }
 
+int orc_set_storage(void* p, int mode, unsigned seed, double param) {
+  Handle* h = (Handle*)p;
+  if (mode < EMU_NONE || mode > EMU_EXM) return -1;
+  auto f = [&](auto* L) { L->storage_mode = mode; L->storage_seed = seed; L->storage_param = param; };
+  if (h->precision) f(h->ld); else f(h->lf);
+  return 0;
+}
+
 int orc_set_threads(int n) {
 #ifdef _OPENMP
   if (n > 0) omp_set_num_threads(n);
@@ -1352,7 +1489,12 @@ int orc_set_densities(void* p, const double* in) {
   Handle* h = (Handle*)p;
   auto f = [&](auto* L) {
     auto& b = L->buf[L->cur];
-    for (size_t i = 0; i < b.size(); i++) b[i] = (decltype(b[0] + 0))in[i];
+    using R = decltype(b[0] + 0);
+    // an emulated 16-bit store rounds to nearest, as the library's host-side conversion does
+    const int mode = L->storage_mode == EMU_F16_SR ? EMU_F16_RN : L->storage_mode == EMU_BF16_SR ? EMU_BF16_RN
+                                                                                                  : L->storage_mode;
+    for (size_t i = 0; i < b.size(); i++)
+      b[i] = mode ? storage_roundtrip(mode, (R)in[i], L->wts[i / L->N], 0u, L->storage_param) : (R)in[i];
   };
   if (h->precision) f(h->ld); else f(h->lf);
   return 0;

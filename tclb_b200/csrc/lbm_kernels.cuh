@@ -374,11 +374,16 @@ struct D3Q19 {
   //   +-x axis:    rho/18 + X/6 - (Y+Z)/6     +-  Jx/6
   //   (sx,sy,0):   rho/36 + (X+Y)/12 + sx*sy*Jx*Jy/(4 rho)  +  (sx*Jx + sy*Jy)/12
   // (and the same with the axes permuted).
-  template <class R>
+  // With EXACT_SUM the rest part is rho - 2 sum(e): the equilibrium then sums
+  // to rho up to the rounding of that sum, not to rho times the rounded
+  // weights' sum (1/3, 1/18, 1/36 are inexact in binary), which as a bias of
+  // ~1e-8 per iteration drifts the mass of a long FP32 run (5000 iterations:
+  // ~2e-4). Deviation storage (rho - 1 in place of rho) does not need it.
+  template <bool EXACT_SUM = false, class R>
   __device__ __forceinline__ static void feq_parts(R rho, R irho, R jx, R jy, R jz, R& e0, R (&e)[9], R (&o)[9]) {
     const R X = jx * jx * irho, Y = jy * jy * irho, Z = jz * jz * irho;
     const R c18 = rho * R(1.0 / 18.0), c36 = rho * R(1.0 / 36.0);
-    e0 = (rho - X - Y - Z) * R(1.0 / 3.0);
+    if (!EXACT_SUM) e0 = (rho - X - Y - Z) * R(1.0 / 3.0);
     e[0] = c18 + (X - Y - Z) * R(1.0 / 6.0);
     e[1] = c18 + (Y - X - Z) * R(1.0 / 6.0);
     e[2] = c18 + (Z - X - Y) * R(1.0 / 6.0);
@@ -400,6 +405,7 @@ struct D3Q19 {
     o[6] = (jz - jx) * R(1.0 / 12.0);
     o[7] = (jy + jz) * R(1.0 / 12.0);
     o[8] = (jz - jy) * R(1.0 / 12.0);
+    if (EXACT_SUM) e0 = rho - R(2) * ((e[0] + e[1] + e[2]) + ((e[3] + e[4]) + (e[5] + e[6]) + (e[7] + e[8])));
   }
 
   // CollisionMRT (:223-290). The d'Humieres rates of TCLB's d3q19 give every
@@ -432,12 +438,12 @@ struct D3Q19 {
     const V rho_t = DEV ? rho + V(1) : rho;  // true density
     const V irho = recip(rho_t);
     V e0, e[9], o[9];
-    feq_parts(rho, irho, jx, jy, jz, e0, e, o);
+    feq_parts<!DEV>(rho, irho, jx, jy, jz, e0, e, o);
     jx += rho_t * V(a.s[d3q19::S_ForceX]);
     jy += rho_t * V(a.s[d3q19::S_ForceY]);
     jz += rho_t * V(a.s[d3q19::S_ForceZ]);
     V e0n, en[9], on[9];
-    feq_parts(rho, irho, jx, jy, jz, e0n, en, on);
+    feq_parts<!DEV>(rho, irho, jx, jy, jz, e0n, en, on);
     f[0] = e0n + g1 * (f[0] - e0);
 #pragma unroll
     for (int p = 0; p < 9; p++) {
