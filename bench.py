@@ -12,6 +12,13 @@ host buffers: each e2e step uploads the initial snapshot from pinned host
 memory, runs the full 2000-iteration case with the same diagnostics every 50,
 and reads the velocity field back.
 
+At N=1 the line also carries ``storage_variants``: the same workload with
+FP16-shift storage (the tile-staged kernel) and in FP64, each timed on the
+device like the headline (MLUPS, the iteration kernel's fraction of the
+measured HBM bandwidth, the ratio to the FP32 line), and each storage's
+relative L2 velocity error against the FP64 run after 2000 iterations from the
+same initial state.
+
 Multi-GPU (torchrun, one rank per GPU): independent replicas, weak scaling, no
 data-path collective (the case does not shard across GPUs here).
 
@@ -56,10 +63,21 @@ def parse():
     p.add_argument("--cpu-slab", type=int, default=16, help="z extent of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--variants", default="fp16s,fp64",
+                   help="N=1: storage variants timed after the headline on the same workload "
+                        "(comma list of fp16s, bf16s, fp64; empty for none)")
+    p.add_argument("--variant-steps", type=int, default=10)
+    p.add_argument("--accuracy-iters", type=int, default=2000,
+                   help="iterations of the accuracy run of each variant (and FP32) against FP64; 0 for none")
     p.add_argument("--rate", type=float, default=6.0, help="config 5: Poisson arrival rate (requests/s)")
     p.add_argument("--path", default="auto", choices=["auto", "tma", "pairs", "one"],
                    help="16-bit storage kernel for plain iterations: auto (tile-staged TMA where it "
                         "applies, else two nodes per thread), tma, pairs, one (one node per thread)")
+    p.add_argument("--case", default="tgv", choices=["tgv", "porous"],
+                   help="timed lattice: the Taylor-Green vortex (the headline) or, with --shape, the d3q19 porous "
+                        "channel of configuration 3 (Bernoulli(0.08) solids, ForceX 1e-6, nu 0.01) for profiling")
+    p.add_argument("--shape", default="", help="nx,ny,nz of a --case porous lattice (default 384,192,192)")
+    p.add_argument("--porosity", type=float, default=0.08, help="solid fraction of a --case porous lattice")
     p.add_argument("--config", type=int, default=2,
                    help="2 = the headline Taylor-Green line; 1, 3, 4, 5 = the other configurations (one JSON line)")
     p.add_argument("--accuracy", action="store_true",
@@ -167,6 +185,26 @@ def tgv_setup(lat, n, u0=0.05, nu=None):
     lat.init_equilibrium(rho, u)
 
 
+def case_lattice(args, precision=None, storage=None):
+    """The timed lattice of --case, set up and resident on the current device."""
+    from tclb_b200 import cases
+    from tclb_b200.lattice import Lattice
+
+    precision, storage = precision or args.precision, storage or args.storage
+    if args.case == "tgv":
+        n = args.n
+        lat = Lattice(args.model, n, n, n, precision=precision, storage=storage)
+        tgv_setup(lat, n)
+        return lat
+    nx, ny, nz = (int(v) for v in (args.shape or "384,192,192").split(","))
+    lat = Lattice("d3q19", nx, ny, nz, precision=precision, storage=storage)
+    lat.set_flags(cases.porous_channel_d3q19(nx, ny, nz, p=args.porosity, band=4, seed=0))
+    lat.SetSetting("nu", 0.01)
+    lat.SetSetting("ForceX", 1e-6)
+    lat.Init()
+    return lat
+
+
 def cpu_baseline(args, model_name, seconds, threads=None):
     """The oracle (CPU restatement of the reference path) on a slab of the
     workload: 256 x 256 x cpu_slab nodes, periodic, same settings."""
@@ -207,6 +245,12 @@ def workload_config(args, world: int) -> dict:
     """The workload both arms report (the reference arm times bounded samples of it)."""
     from tclb_b200 import models as M
 
+    if args.case == "porous":
+        nx, ny, nz = (int(v) for v in (args.shape or "384,192,192").split(","))
+        return {"workload": f"d3q19 porous channel {nx}x{ny}x{nz}, Bernoulli({args.porosity:g}) solids, ForceX=1e-6, "
+                            "nu=0.01",
+                "model": "d3q19", "lattice": [nx, ny, nz], "precision": args.precision, "storage": args.storage,
+                "iterations_per_step": args.log_every, "parallelism": f"replicas x{world}"}
     m = M.get(args.model)
     n = args.n
     elem = 8 if args.precision == "fp64" else (4 if args.storage == "same" else 2)
@@ -249,6 +293,91 @@ def run_reference(args):
     return 0
 
 
+def timed_steps(lat, steps, I, stream):
+    """K logging steps (I-1 plain iterations, one with Globals, the energy/enstrophy reduction) timed with
+    CUDA events on the launching stream: (total seconds, mean plain-iteration seconds, last energy)."""
+    import torch
+
+    from tclb_b200 import models as M
+
+    sp = stream.cuda_stream
+    pairs = []
+    energy = (0.0, 0.0)
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
+        b.record(stream)
+        lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
+        energy = lat.energy_enstrophy(stream=sp)
+        pairs.append((a, b))
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    t = e_start.elapsed_time(e_end) / 1e3
+    kern = sum(a.elapsed_time(b) for a, b in pairs) / 1e3 / (steps * (I - 1))
+    return t, kern, energy
+
+
+def kernel_name(path) -> str:
+    return "k_iterate_tma" if path["tma"] else ("k_iterate_pair" if path["pairs"] else "k_iterate")
+
+
+def storage_variants(args, stream, fp32_value, fp32_kern):
+    """The headline workload with other storage: FP16-shift (tile-staged kernel), BF16-shift, FP64.
+    Each: MLUPS over --variant-steps logging steps (lattice resident), its plain-iteration kernel's
+    fraction of the measured HBM bandwidth, the ratio to the FP32 line; then the relative L2 velocity
+    error of each storage (and of FP32) against FP64 after --accuracy-iters iterations."""
+    import torch
+
+    from tclb_b200 import models as M
+    from tclb_b200.lattice import Lattice
+
+    n, I = args.n, args.log_every
+    peaks, _ = measured_peaks()
+    names = [v for v in args.variants.split(",") if v]
+    out = {}
+    for v in names:
+        prec, sto = ("fp64", "same") if v == "fp64" else ("fp32", v)
+        lat = Lattice(args.model, n, n, n, precision=prec, storage=sto)
+        tgv_setup(lat, n)
+        for _ in range(3):
+            timed_steps(lat, 1, I, stream)
+        clocks = ClockSampler(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+        clocks.start()
+        time.sleep(0.2)
+        t, kern, _ = timed_steps(lat, args.variant_steps, I, stream)
+        clk = clocks.stop()
+        bpu = lat.bytes_per_update
+        value = lat.N * I * args.variant_steps / t / 1e6
+        out[v] = {"precision": prec, "storage": sto, "value": value, "unit": UNIT,
+                  "kernel": kernel_name(lat.launch_path()), "kernel_mlups": lat.N / kern / 1e6,
+                  "bytes_per_update": bpu, "frac": bpu * lat.N / kern / 1e9 / peaks["hbm_gbs"],
+                  "ratio_vs_fp32": value / fp32_value, "kernel_ratio_vs_fp32": fp32_kern / kern,
+                  "steps": args.variant_steps, "sm_mhz": clk.get("sm_mhz"), "clock_reasons": clk.get("reasons")}
+        lat.close()
+    if args.accuracy_iters > 0:
+        u = {}
+        for v in ["fp64", "fp32"] + [x for x in names if x != "fp64"]:
+            prec, sto = ("fp64", "same") if v == "fp64" else ("fp32", "same" if v == "fp32" else v)
+            lat = Lattice(args.model, n, n, n, precision=prec, storage=sto)
+            tgv_setup(lat, n)
+            lat.Iterate(args.accuracy_iters, M.ITER_NORM, stream=stream.cuda_stream)
+            u[v] = lat.GetQuantity("U", stream=stream.cuda_stream).astype(np.float64)
+            lat.close()
+        ref = u["fp64"]
+        nrm = float(np.linalg.norm(ref))
+        for v, uv in u.items():
+            if v == "fp64":
+                continue
+            err = float(np.linalg.norm(uv - ref) / nrm)
+            out.setdefault(v, {})["velocity_rel_l2_vs_fp64"] = err
+        out["accuracy_run"] = f"{args.accuracy_iters} iterations from the same initial state, U against FP64"
+    torch.cuda.synchronize()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -269,12 +398,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, args.model, args.cpu_seconds)
 
-    lat = Lattice(args.model, n, n, n, precision=args.precision, storage=args.storage)
+    lat = case_lattice(args)
     if args.path != "auto":
-        lat.set_launch(128 if n >= 128 else 32, 2 if n >= 128 else 8, use_graphs=True,
+        lat.set_launch(128 if lat.nx >= 128 else 32, 2 if lat.nx >= 128 else 8, use_graphs=True,
                        use_pairs=args.path in ("pairs", "tma"), use_tma=args.path == "tma")
     path = lat.launch_path()
-    tgv_setup(lat, n)
     # a dedicated (non-default) stream: the library launches on it, the CUDA
     # events below are recorded on it
     stream = torch.cuda.Stream()
@@ -293,26 +421,13 @@ def run_ours(args):
     clocks = ClockSampler(phys)
     clocks.start()
     time.sleep(0.3)
-    pairs = []
     t_wall0 = time.perf_counter()
-    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
-    e_start.record(stream)
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        lat.Iterate(I - 1, M.ITER_NORM, stream=sp)
-        b.record(stream)
-        lat.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sp)
-        energy = lat.energy_enstrophy(stream=sp)  # kinetic energy and enstrophy every I iterations
-        pairs.append((a, b))
-    e_end.record(stream)
-    torch.cuda.synchronize()
+    # kinetic energy and enstrophy every I iterations
+    t, kern, energy = timed_steps(lat, args.steps, I, stream)
     barrier()
     wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
-    t = e_start.elapsed_time(e_end) / 1e3
-    kern = sum(a.elapsed_time(b) for a, b in pairs) / 1e3 / (args.steps * (I - 1))
     kern = reduce_max(kern)
     glob = lat.globals_dict()
     updates = N * I * args.steps
@@ -320,8 +435,8 @@ def run_ours(args):
 
     peaks, peak_src = measured_peaks()
     achieved = bpu * N / kern / 1e9
-    kernel = "k_iterate_tma" if path["tma"] else ("k_iterate_pair" if path["pairs"] else "k_iterate")
-    traffic = profiled_traffic(kernel, args.model, args.precision, args.storage, n)
+    kernel = kernel_name(path)
+    traffic = profiled_traffic(kernel, args.model, args.precision, args.storage, n) if args.case == "tgv" else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_src,
             "kernel": kernel + (" (no-Globals variant)" if kernel == "k_iterate" else ""), "bytes_per_update": bpu,
@@ -357,6 +472,11 @@ def run_ours(args):
                "step": "upload snapshot (pinned), full case with Globals, kinetic energy and enstrophy every "
                        "50 iterations, read U back"}
 
+    lat.close()
+    variants = None
+    if world == 1 and args.variants and args.storage == "same" and args.precision == "fp32" and args.case == "tgv":
+        variants = storage_variants(args, stream, value, kern)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
@@ -364,11 +484,10 @@ def run_ours(args):
                 "config": workload_config(args, world),
                 "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one"),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-                "gpu_launches": args.steps * (I + 2), "wall_s": wall,
+                "gpu_launches": args.steps * (I + 2), "wall_s": wall, "storage_variants": variants,
                 "globals_last": dict({k: float(v) for k, v in glob.items()}, KineticEnergy=energy[0],
                                      Enstrophy=energy[1])}
         print(json.dumps(line), flush=True)
-    lat.close()
     reps.close()
     return 0
 

@@ -141,10 +141,12 @@ int tclb_energy_enstrophy(tclb_h h, double* out, void* stream);
    library (held by every GPU that loads the library until the process exits)
    and calls no cudaMalloc/cudaFree. Regions whose quantity needs more than
    8 MiB (nodes x components x sizeof(real_t)) are rejected with
-   TCLB_ERR_ARG. The first call on a device looks up the array's device
-   address (cudaGetSymbolAddress) and caches it; make that first call before
-   any stream capture. All calls share the array: calls that overlap on the
-   GPU race. */
+   TCLB_ERR_ARG. The call ends by synchronising its stream, so it cannot be
+   captured into a CUDA graph. The first call on each device looks up the
+   array's device address (cudaGetSymbolAddress) and caches it; make that
+   first call before another thread of the process starts a global-mode
+   stream capture. All calls share the array: calls that overlap on the GPU
+   race. */
 int tclb_get_quantity_noalloc(tclb_h h, int q, const int region[6], void* out, double scale, void* stream);
 
 /* Get_/Set_<field> for all densities at once: SoA [q][z][y][x] as double. */
@@ -184,7 +186,8 @@ int tclb_sync(tclb_h h);
    collision for both (on by default); TCLB_LAUNCH_TMA lets 16-bit storage
    stage tiles of whole rows in shared memory with TMA on plain iterations
    (on by default; it takes precedence over PAIRS) when nx is a multiple of 64
-   up to 256 and ny a multiple of 512/nx. bx, by shape the one-node kernel.
+   up to 512 and ny a multiple of floor(512/nx). bx, by shape the one-node
+   kernel.
    A staging wait that runs out (about a second) is reported as TCLB_ERR_CUDA
    by the next tclb_sync or Globals-reading tclb_iterate. */
 #define TCLB_LAUNCH_GRAPHS 1
@@ -194,6 +197,16 @@ int tclb_set_launch(tclb_h h, int bx, int by, int flags);
 /* The launch shape and the paths plain iterations take on this lattice: the
    flags that are both enabled and applicable (no TCLB counterpart). */
 int tclb_get_launch(tclb_h h, int* bx, int* by, int* flags);
+/* Failure-path test of the tile-staged kernel (no TCLB counterpart; TCLB
+   exits on a CUDA error, src/cross.cu:24-32): plain iterations run with
+   every staging wait bounded by wait_cycles SM clock cycles (0: the default,
+   about a second) and, when tile >= 0, the producer arms that tile's stage
+   without issuing its copies, so the wait of its consumers runs out. The
+   iteration then leaves that tile's nodes unwritten, and the next tclb_sync
+   returns TCLB_ERR_CUDA, reports it in tclb_last_error() and clears the
+   device error word. tile = -1 and wait_cycles = 0 restore normal runs.
+   Nothing faults: the kernel returns after its bounded waits. */
+int tclb_set_fault_injection(tclb_h h, int tile, long long wait_cycles);
 
 /* ---------------------------------------------------------------------------
    XML case files (<CLBConfig>): the control flow of TCLB's main and handler
@@ -263,7 +276,7 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    (blocks of bx / 2 x min(by, T / (bx / 2)) threads, T = 256, 128 for
    d3q27_cumulant); the Globals launch keeps the one-node kernel.
    TCLB_LAUNCH_TMA (on by default) runs the plain launches of each 16-bit case
-   whose rows fit one TMA box (nx a multiple of 64 up to 256, 512 / nx
+   whose rows fit one TMA box (nx a multiple of 64 up to 512, floor(512 / nx)
    dividing ny) through the tile-staged kernel, tensor maps kept with the case;
    the other cases take the pair or one-node form. A staging wait that runs
    out (about a second) is reported as TCLB_ERR_CUDA by the next

@@ -564,37 +564,39 @@ static inline float round_fixed(float g, double w, double scale) {
 
 // h = g / w in a 16-bit float with E exponent bits, 15 - E mantissa bits and top S (param = E * 16 + log2(1/S)):
 // binades [S 2^-k-1, S 2^-k) for k < 2^E - 1, then a subnormal range of spacing S 2^-(2^E - 1) 2^-(15-E).
-static inline float round_exm(float g, double w, double param) {
+static inline double round_exm_d(double g, double w, double param) {
   const int E = (int)param / 16, L = (int)param % 16, M = 15 - E;
   const double S = std::ldexp(1.0, -L), h = (double)g / w, a = std::fabs(h);
   const int nb = (1 << E) - 1;  // normal binades
   int k = 0;                    // binade below the top
   double unit;
-  if (a >= S) return (float)(std::copysign(S - std::ldexp(S, -1 - M), h) * w);  // saturate (not reached here)
+  if (a >= S) return std::copysign(S - std::ldexp(S, -1 - M), h) * w;  // saturate
   if (E == 0) unit = std::ldexp(S, -M);
   else {
     while (k < nb && a < std::ldexp(S, -1 - k)) k++;
     unit = k < nb ? std::ldexp(S, -1 - k - M) : std::ldexp(S, -nb - M);
   }
   const double q = std::nearbyint(a / unit) * unit;
-  return (float)(std::copysign(std::min(q, S - std::ldexp(S, -1 - M)), h) * w);
+  return std::copysign(std::min(q, S - std::ldexp(S, -1 - M)), h) * w;
 }
 
 template <class R>
 static inline R storage_roundtrip(int mode, R f, double w, uint32_t rnd, double param = 0) {
-  const float wf = (float)w, g = (float)f - wf;
+  // the deviation in the oracle's arithmetic, then rounded to the format
+  const R wr = (R)w;
+  const float g = (float)(f - wr);
   float d;
   switch (mode) {
     case EMU_MANT: d = round_mantissa(g, (int)param); break;
     case EMU_FIXED: d = round_fixed(g, w, param); break;
-    case EMU_EXM: d = round_exm(g, w, param); break;
+    case EMU_EXM: return (R)round_exm_d((double)(f - wr), w, param) + wr;
     case EMU_F16_RN: d = f16_to_f32(f32_to_f16(g, false, 0)); break;
     case EMU_F16_SR: d = f16_to_f32(f32_to_f16(g, true, rnd)); break;
     case EMU_BF16_RN: d = bf16_to_f32(f32_to_bf16(g, false, 0)); break;
     case EMU_BF16_SR: d = bf16_to_f32(f32_to_bf16(g, true, rnd)); break;
     default: return f;
   }
-  return (R)(d + wf);
+  return (R)d + wr;
 }
 
 struct GlobAcc {

@@ -298,6 +298,11 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150,
         agg = aggregate_serving(reps, rep, [r.finished - r.arrival for r in done], sum(r.updates for r in done),
                                 t_ideal)
         agg["single_large_case_MLUPS"] = single
+        if reps.world == 1:  # where the busy time went (one server)
+            agg["busy_by_model_s"] = rep["busy_by_model_s"]
+            agg["busy_all_models_s"] = rep["busy_all_models_s"]
+            agg["model_mlups_while_in_flight"] = {
+                m: rep["updates_by_model"][m] / t / 1e6 for m, t in rep["busy_by_model_s"].items() if t > 0}
         out["runs"][st] = agg
     return out
 

@@ -8,6 +8,7 @@
 // (src/Handlers/acSolve.cpp:5-43, vHandler.h:69-87). Output names follow
 // Solver::outIterFile (src/Solver.h.Rt:102-105).
 #include <sys/stat.h>
+#include <zlib.h>
 
 #include <algorithm>
 #include <array>
@@ -1107,8 +1108,8 @@ struct Runner {
   // units and the lattice size, and one text file per quantity (`what`,
   // default all) in SI units: %.8g (float) or %.16lg (double) values, a new
   // line after every nx nodes. Vector quantities give x y z per node (TCLB
-  // reads them into a one-value-per-node buffer). gzip="true" pipes each
-  // quantity file through gzip into <file>.gz.
+  // reads them into a one-value-per-node buffer). gzip="true" writes each
+  // quantity file gzip-compressed (zlib) as <file>.gz.
   void write_txt(const Callback& c) {
     int nx, ny, nz;
     tclb_get_size(lat, &nx, &ny, &nz);
@@ -1140,26 +1141,57 @@ struct Runner {
       const int comp = T->quantity_vector[q] ? 3 : 1;
       std::vector<char> buf(size * comp * (dbl ? 8 : 4));
       ck(tclb_get_quantity(lat, q, nullptr, buf.data(), si_scale(model, qn), nullptr), "quantity");
-      const std::string fn = base + "_" + qn + ".txt";
-      // the file name goes to the shell inside single quotes, so it may not hold one
-      if (gzip && fn.find('\'') != std::string::npos) throw CaseError("<TXT gzip>: quote in file name " + fn);
-      FILE* f = gzip ? popen(("gzip > '" + fn + ".gz'").c_str(), "w") : std::fopen(fn.c_str(), "w");
-      if (!f) throw CaseError("cannot write " + fn);
+      const std::string fn = base + "_" + qn + ".txt" + (gzip ? ".gz" : "");
+      TextSink out(fn, gzip);
+      char num[40];
       for (size_t i = 0; i < size; i++) {
         for (int k = 0; k < comp; k++) {
-          if (k) std::fputc(' ', f);
-          if (dbl) std::fprintf(f, "%.16lg", reinterpret_cast<const double*>(buf.data())[i * comp + k]);
-          else std::fprintf(f, "%.8g", (double)reinterpret_cast<const float*>(buf.data())[i * comp + k]);
+          if (k) out.put(" ", 1);
+          const int len = dbl ? std::snprintf(num, sizeof(num), "%.16lg", reinterpret_cast<const double*>(buf.data())[i * comp + k])
+                              : std::snprintf(num, sizeof(num), "%.8g",
+                                              (double)reinterpret_cast<const float*>(buf.data())[i * comp + k]);
+          out.put(num, (size_t)len);
         }
-        std::fputc((i + 1) % nx == 0 ? '\n' : ' ', f);
+        out.put((i + 1) % nx == 0 ? "\n" : " ", 1);
       }
-      if (gzip) {
-        if (pclose(f) != 0) throw CaseError("gzip failed for " + fn);
-      } else {
-        std::fclose(f);
-      }
+      out.close();
     }
   }
+
+  // A text file written through a buffer, plain or gzip-compressed (zlib).
+  struct TextSink {
+    std::string name, buf;
+    FILE* f = nullptr;
+    gzFile z = nullptr;
+    TextSink(const std::string& fn, bool gzip) : name(fn) {
+      if (gzip) z = gzopen(fn.c_str(), "wb");
+      else f = std::fopen(fn.c_str(), "w");
+      if (!f && !z) throw CaseError("cannot write " + fn);
+      buf.reserve(1 << 20);
+    }
+    ~TextSink() {
+      if (f) std::fclose(f);
+      if (z) gzclose(z);
+    }
+    void put(const char* p, size_t n) {
+      buf.append(p, n);
+      if (buf.size() >= (1u << 20)) flush();
+    }
+    void flush() {
+      if (buf.empty()) return;
+      const bool ok = f ? std::fwrite(buf.data(), 1, buf.size(), f) == buf.size()
+                        : gzwrite(z, buf.data(), (unsigned)buf.size()) == (int)buf.size();
+      if (!ok) throw CaseError("write failed for " + name);
+      buf.clear();
+    }
+    void close() {
+      flush();
+      const bool ok = f ? std::fclose(f) == 0 : gzclose(z) == Z_OK;
+      f = nullptr;
+      z = nullptr;
+      if (!ok) throw CaseError("write failed for " + name);
+    }
+  };
 
   // binWriteLattice (src/vtkLattice.cpp:58-81): one raw real_t file per quantity
   void write_bin(const std::string& prefix) {

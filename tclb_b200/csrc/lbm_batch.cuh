@@ -319,7 +319,10 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       if (lane == 0 && n >= S) ok = mbar_wait(smem_u32(&empty[s]), (unsigned)(n / S - 1) & 1u);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) {
-        if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
+        if (lane == 0) {
+          atomicExch(err, TMA_ERR_TIMEOUT);
+          tma_drain(full, S, n, TMA_WAIT_CYCLES);
+        }
         return;
       }
       if (lane == 0) {

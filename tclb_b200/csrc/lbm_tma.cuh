@@ -39,13 +39,18 @@ struct TmaMaps {
 };
 
 // Rows per tile of a lattice for the tile-staged kernels: 16-bit storage, nx
-// a multiple of 64 up to 256 (a row is one TMA box), R = 512 / nx dividing
-// ny; 0 where they do not apply.
+// a multiple of 64 up to 512, R = floor(512 / nx) rows dividing ny; 0 where
+// they do not apply. A row is one TMA box: up to 256 values as one box row
+// (TMA boxes are at most 256 values along a dimension), wider rows as a
+// (64, nx/64) box of a tensor whose x axis is split in two (64 x nx/64), which
+// lands in shared memory in the same row-major order.
+constexpr int TMA_MAX_NX = 512;
 inline int tma_rows_for(size_t elem, int nx, int ny) {
-  if (elem != 2 || nx % 64 || nx > 256) return 0;
+  if (elem != 2 || nx % 64 || nx > TMA_MAX_NX) return 0;
   const int R = 512 / nx;
   return ny % R ? 0 : R;
 }
+__host__ __device__ inline bool tma_wide(int nx) { return nx > 256; }
 
 // The driver's cuTensorMapEncodeTiled, reached through the runtime's
 // entry-point query so the library links only the runtime; null if absent.
@@ -76,6 +81,28 @@ inline bool encode_tile_maps(void* buf, const void* flags, int nx, int ny, int n
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return false;
   const cuuint64_t e = 2;
+  if (tma_wide(nx)) {  // x split as (64, nx/64): rows (64, nx/64, ny, nz, Q), node types (64, nx/64, ny, nz)
+    const cuuint32_t xo = (cuuint32_t)(nx / 64);
+    const cuuint64_t dims[5] = {64, xo, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
+    const cuuint64_t strides[4] = {64 * e, nx * e, (cuuint64_t)nx * ny * e, stride * e};
+    const cuuint32_t box_rows[5] = {64, xo, (cuuint32_t)R, 1, 1};
+    const cuuint32_t box_row1[5] = {64, xo, 1, 1, 1};
+    const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+    if (enc(rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 5, buf, dims, strides, box_rows, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    if (enc(row1, CU_TENSOR_MAP_DATA_TYPE_UINT16, 5, buf, dims, strides, box_row1, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    const cuuint64_t fdims[4] = {64, xo, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t fstrides[3] = {64 * e, nx * e, (cuuint64_t)nx * ny * e};
+    const cuuint32_t fbox[4] = {64, xo, (cuuint32_t)R, 1};
+    return enc(fmap, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, const_cast<void*>(flags), fdims, fstrides, fbox, ones,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
   const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
   const cuuint64_t strides[3] = {nx * e, (cuuint64_t)nx * ny * e, stride * e};
   const cuuint32_t box_rows[4] = {(cuuint32_t)nx, (cuuint32_t)R, 1, 1};
@@ -131,7 +158,7 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
 }
 
 // Bounded wait for the phase with the given parity; false when it ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, long long limit = TMA_WAIT_CYCLES) {
   const long long t0 = clock64();
   for (;;) {
     unsigned done;
@@ -143,8 +170,17 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > TMA_WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
+}
+
+// A producer leaving on a timeout first waits (bounded again) for the copies
+// it issued into the other stages -- those of the tiles n-S+1 .. n-1, armed
+// last -- so that none is still in flight into shared memory when the block
+// exits. A stage whose copies were never issued just runs out once more.
+__device__ __forceinline__ void tma_drain(unsigned long long* full, int S, int n, long long limit) {
+  for (int j = n - S + 1 < 0 ? 0 : n - S + 1; j < n; j++)
+    mbar_wait(static_cast<unsigned>(__cvta_generic_to_shared(&full[j % S])), (unsigned)(j / S) & 1u, limit);
 }
 
 __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -153,6 +189,15 @@ __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map
       "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
       "[%6];" ::"r"(dst),
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            int c4, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
       : "memory");
 }
 
@@ -178,6 +223,7 @@ __device__ __forceinline__ void tma_fill_at(const CUtensorMap* rows, const CUten
                                             const CUtensorMap* flags, unsigned short* stage, unsigned bar, int z,
                                             int y0, int nx, int ny, int nz, int R, int lane) {
   constexpr unsigned block = TMA_TILE;  // values per population block (R * nx at most)
+  const bool wide = tma_wide(nx);        // coordinates (0, 0, y, z, i) of the split-x maps
   if (lane < M::Q) {
     const int i = lane;
     const int ey = M::ey(i), ez = M::DIM == 2 ? 0 : M::ez(i);
@@ -186,16 +232,19 @@ __device__ __forceinline__ void tma_fill_at(const CUtensorMap* rows, const CUten
     const unsigned dst = smem_u32(stage + (size_t)i * block);
     const int ys = y0 - ey;
     if (ys >= 0 && ys + R <= ny) {
-      tma_load_4d(dst, rows, 0, ys, zs, i, bar);
+      if (wide) tma_load_5d(dst, rows, 0, 0, ys, zs, i, bar);
+      else tma_load_4d(dst, rows, 0, ys, zs, i, bar);
     } else {  // rows wrap at a y face: one row at a time
       for (int r = 0; r < R; r++) {
         int y = ys + r;
         y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-        tma_load_4d(dst + (unsigned)(r * nx * 2), row1, 0, y, zs, i, bar);
+        if (wide) tma_load_5d(dst + (unsigned)(r * nx * 2), row1, 0, 0, y, zs, i, bar);
+        else tma_load_4d(dst + (unsigned)(r * nx * 2), row1, 0, y, zs, i, bar);
       }
     }
   } else if (lane == M::Q) {
-    tma_load_3d(smem_u32(stage + (size_t)M::Q * block), flags, 0, y0, z, bar);
+    if (wide) tma_load_4d(smem_u32(stage + (size_t)M::Q * block), flags, 0, 0, y0, z, bar);
+    else tma_load_3d(smem_u32(stage + (size_t)M::Q * block), flags, 0, y0, z, bar);
   }
 }
 
@@ -216,10 +265,17 @@ __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage
 // TMA_STAGES stages.
 constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
 
-template <class M, class R, class St>
+// FAULT (the failure-path test, set only by tclb_set_fault_injection):
+// wait_cycles bounds every mbarrier wait instead of the fixed bound, and the
+// producer arms tile skip_tile's stage but issues none of its copies, so its
+// consumers' wait runs out. Without FAULT both parameters are ignored and
+// the waits keep the compile-time bound.
+template <class M, class R, class St, bool FAULT = false>
 __global__ void __launch_bounds__(TMA_THREADS, 2)
     k_iterate_tma(const Args<R, M::NSET> a, const __grid_constant__ TmaMaps T,
-                  const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err) {
+                  const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err, long long wait_cycles_arg,
+                  int skip_tile) {
+  const long long wait_cycles = FAULT ? wait_cycles_arg : TMA_WAIT_CYCLES;
   static_assert(M::Q < 32, "one producer lane per population plus one for the node types");
   using P16 = Pack16<St>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -252,10 +308,14 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       const int s = k % TMA_STAGES;
       const unsigned fb = smem_u32(&full[s]);
       bool ok = true;
-      if (lane == 0 && k >= TMA_STAGES) ok = mbar_wait(smem_u32(&empty[s]), (unsigned)(k / TMA_STAGES - 1) & 1u);
+      if (lane == 0 && k >= TMA_STAGES)
+        ok = mbar_wait(smem_u32(&empty[s]), (unsigned)(k / TMA_STAGES - 1) & 1u, wait_cycles);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) {
-        if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
+        if (lane == 0) {
+          atomicExch(err, TMA_ERR_TIMEOUT);
+          tma_drain(full, TMA_STAGES, k, wait_cycles);
+        }
         return;
       }
       if (lane == 0) {
@@ -263,7 +323,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
         mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(R_rows * nx) * 2u);  // the bytes of R_rows rows
       }
       __syncwarp();
-      tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);
+      if (!FAULT || t != skip_tile) tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);
     }
     return;
   }
@@ -279,7 +339,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   int s = 0;
   unsigned phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const bool ok = mbar_wait(smem_u32(&full[s]), phase);
+    const bool ok = mbar_wait(smem_u32(&full[s]), phase, wait_cycles);
     if (!__all_sync(0xffffffffu, ok)) {  // the warp leaves together
       if (lane == 0) atomicExch(err, TMA_ERR_TIMEOUT);
       return;

@@ -163,6 +163,10 @@ struct tclb_lattice {
   int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_grid = 0;
   TmaMaps tma[2];
   int* err_dev = nullptr;
+  // failure-path test of the tile-staged kernel (tclb_set_fault_injection):
+  // the tile whose copies are not issued (-1: none) and the wait bound
+  int fault_tile = -1;
+  long long wait_cycles = TMA_WAIT_CYCLES;
 };
 
 struct Impl {
@@ -221,7 +225,12 @@ struct Launch {
         const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
         const size_t smem = tma_smem_bytes<M>();
         if (L->tma_grid > 0) {
-          k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev);
+          if (L->fault_tile >= 0 || L->wait_cycles != TMA_WAIT_CYCLES)  // the failure-path test
+            k_iterate_tma<M, R, St, true><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev,
+                                                                            L->wait_cycles, L->fault_tile);
+          else
+            k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev,
+                                                                        TMA_WAIT_CYCLES, -1);
           return;
         }
       }
@@ -248,8 +257,14 @@ struct Launch {
       const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
       const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
+      // the largest shared-memory carveout: blocks of narrow tiles (224 threads) then fit three per SM
+      // where their registers allow (d3q19), instead of the two the default carveout holds
       if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
               cudaSuccess ||
+          cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+          cudaFuncSetAttribute(k_iterate_tma<M, R, St, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_iterate_tma<M, R, St>, threads, smem) !=
               cudaSuccess ||
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, L->device) != cudaSuccess || per_sm < 1) {
@@ -322,12 +337,12 @@ const Impl* impl_for(int model, int precision, int storage) {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Tensor maps of the tile-staged kernel (16-bit storage, nx a multiple of 64
-// and at most 256, R = 512 / nx rows per tile dividing ny). When anything
-// does not fit, tma_ok stays 0 and the register kernels run.
+// and at most 512, R = floor(512 / nx) rows per tile dividing ny). When
+// anything does not fit, tma_ok stays 0 and the register kernels run.
 void setup_tma(tclb_lattice* L) {
   L->tma_ok = 0;
-  // Tiles of 512 nodes (R whole rows). Longer rows take the register pair
-  // kernel: one-row tiles copied in two boxes measured slower than it.
+  // Tiles of at most 512 nodes (R whole rows; one row when nx > 256, copied
+  // as one split-x box). Longer rows take the register pair kernel.
   const int R = tma_rows_for(L->elem, L->nx, L->ny);
   if (!R) return;
   for (int b = 0; b < 2; b++)
@@ -1021,6 +1036,16 @@ int tclb_set_launch(tclb_h L, int bx, int by, int flags) {
   return TCLB_OK;
 }
 
+int tclb_set_fault_injection(tclb_h L, int tile, long long wait_cycles) {
+  CHECK_H(L);
+  if (tile < -1) return fail(TCLB_ERR_ARG, "fault injection: tile must be -1 (off) or a tile index");
+  if (wait_cycles < 0 || wait_cycles > TMA_WAIT_CYCLES) return fail(TCLB_ERR_ARG, "fault injection: wait bound out of range");
+  drop_graphs(L);  // the kernel parameters are part of the captured launches
+  L->fault_tile = tile;
+  L->wait_cycles = wait_cycles ? wait_cycles : TMA_WAIT_CYCLES;
+  return TCLB_OK;
+}
+
 int tclb_get_launch(tclb_h L, int* bx, int* by, int* flags) {
   CHECK_H(L);
   if (bx) *bx = L->bx;
@@ -1116,6 +1141,11 @@ extern "C" int tclb_get_quantity_noalloc(tclb_h L, int q, const int region[6], v
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = fail(TCLB_ERR_CUDA, std::string("no-allocation quantity: ") + cudaGetErrorString(e));
   }
-  if (prev != L->device) cudaSetDevice(prev);
+  if (prev != L->device) {
+    const cudaError_t e = cudaSetDevice(prev);
+    if (e != cudaSuccess && rc == TCLB_OK)
+      rc = fail(TCLB_ERR_CUDA, std::string("no-allocation quantity: could not restore the caller's device: ") +
+                                   cudaGetErrorString(e));
+  }
   return rc;
 }

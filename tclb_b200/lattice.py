@@ -61,6 +61,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_get_globals.argtypes = [h, dp]
     L.tclb_clear_globals.argtypes = [h]
     L.tclb_get_quantity.argtypes = [h, i, ip, vp, d, vp]
+    L.tclb_get_quantity_noalloc.argtypes = [h, i, ip, vp, d, vp]
     L.tclb_get_densities.argtypes = [h, dp]
     L.tclb_set_densities.argtypes = [h, dp]
     L.tclb_snapshot_bytes.argtypes = [h]
@@ -78,6 +79,7 @@ def load_library(path: Optional[str] = None):
     L.tclb_load_pri.argtypes = [h, vp, sz]
     L.tclb_color.argtypes = [h, vp, i, i, vp]
     L.tclb_get_launch.argtypes = [h, ip, ip, ip]
+    L.tclb_set_fault_injection.argtypes = [h, i, ctypes.c_longlong]
     L.tclb_energy_enstrophy.argtypes = [h, dp, vp]
     _lib = L
     return L
@@ -209,6 +211,21 @@ class Lattice:
 
     quantity = GetQuantity
 
+    def GetQuantityNoAlloc(self, name, region: Optional[Sequence[int]] = None, scale: float = 1.0, out=None,
+                           stream: int = 0) -> np.ndarray:
+        """GetQuantity through tclb_get_quantity_noalloc: no device allocation, the quantity staged in the
+        library's fixed 8 MiB device array (larger regions raise TCLBError; overlapping calls race)."""
+        q = name if isinstance(name, int) else self.model.quantity_index(name)
+        vec = self.model.quantities[q][1]
+        r = list(region) if region is not None else [0, 0, 0, self.nx, self.ny, self.nz]
+        shp = (r[5], r[4], r[3]) + ((3,) if vec else ())
+        if out is None:
+            out = np.zeros(shp, self.real)
+        reg = (ctypes.c_int * 6)(*r)
+        _check(self.lib.tclb_get_quantity_noalloc(self._h, q, reg, ctypes.c_void_p(out.ctypes.data), float(scale),
+                                                  ctypes.c_void_p(stream or None)))
+        return out
+
     def densities(self) -> np.ndarray:
         out = np.zeros((self.model.Q,) + self.shape)
         _check(self.lib.tclb_get_densities(self._h, _dp(out)))
@@ -285,6 +302,11 @@ class Lattice:
         _check(self.lib.tclb_get_launch(self._h, ctypes.byref(bx), ctypes.byref(by), ctypes.byref(fl)))
         return {"bx": bx.value, "by": by.value, "graphs": bool(fl.value & 1), "pairs": bool(fl.value & 2),
                 "tma": bool(fl.value & 4)}
+
+    def set_fault_injection(self, tile: int = -1, wait_cycles: int = 0):
+        """Failure-path test of the tile-staged kernel: skip the copies of one tile and bound every staging
+        wait by wait_cycles clock cycles; the next sync() raises TCLBError. tile=-1, wait_cycles=0: off."""
+        _check(self.lib.tclb_set_fault_injection(self._h, int(tile), int(wait_cycles)))
 
     def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True, use_tma: bool = True):
         flags = (1 if use_graphs else 0) | (2 if use_pairs else 0) | (4 if use_tma else 0)

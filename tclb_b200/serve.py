@@ -1,14 +1,21 @@
 """Continuous-batching request loop over tclb_batch.
 
 Requests (a case of some model: node types, settings, iterations) arrive over
-time. The loop admits queued requests in arrival order while their device
-footprint fits the memory budget and keeps admitted lattices resident. Each
-model has one batch on its own stream; the batches run independently: as soon
-as a batch's graph replay has finished (a non-blocking query), its finished
-cases are retired (Globals and, on request, a quantity are read back), waiting
-requests are admitted into it, and its next replay is enqueued -- so the
-models' work overlaps on the GPU and no batch waits for another. Time to
-solution = completion time - arrival time.
+time. Admission (`Admission`, host logic only) keeps one FIFO queue per model
+under one device-memory budget: a request is admitted when it has arrived and
+its footprint fits; one that waits for memory does not hold up the other
+models' requests unless it has waited longer than a bound, after which
+nothing younger goes ahead of it. An admitted request is reserved at once; it
+joins its model's batch at the batch's next replay boundary (a pending list),
+so admission never waits for a replay in flight. Admitted lattices stay
+resident. Each model has one batch on its own stream and the batches run
+independently: when a batch's graph replay has finished (a non-blocking
+query), its finished and cancelled cases are retired (Globals and, on
+request, a quantity are read back for finished ones), its pending cases join,
+and its next replay is enqueued -- so the models' work overlaps on the GPU.
+A request can be cancelled while it waits, while it is pending, or while it
+runs (it leaves at its batch's next boundary). Time to solution = completion
+time - arrival time.
 
 No counterpart in the reference (TCLB runs one case per process).
 """
@@ -17,7 +24,7 @@ from __future__ import annotations
 import time
 from collections import deque
 from dataclasses import dataclass, field
-from typing import Callable, Deque, Dict, List, Optional, Tuple
+from typing import Callable, Deque, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -35,6 +42,7 @@ class Request:
     # filled in by the server
     admitted: float = -1.0
     finished: float = -1.0
+    cancelled: bool = False
     globals: Optional[np.ndarray] = None
     quantity: Optional[np.ndarray] = None
 
@@ -47,10 +55,71 @@ class Request:
         return self.nodes * self.spec.niter
 
 
+class Admission:
+    """Admission under one device-memory budget, one FIFO queue per model.
+
+    `admit(now)` takes the queue heads that have arrived, oldest first, and
+    admits each whose footprint fits what is left of the budget. A head that
+    does not fit leaves the other queues free to go on -- unless it has been
+    waiting for memory for `max_bypass_s` or longer: then nothing else is
+    admitted until it fits (no request starves behind a stream of smaller
+    ones). `release` returns a finished or cancelled request's memory.
+    """
+
+    def __init__(self, budget_bytes: int, footprint: Callable[[Request], int], models=(), max_bypass_s: float = 5.0):
+        self.budget = int(budget_bytes)
+        self.footprint = footprint
+        self.max_bypass_s = float(max_bypass_s)
+        self.queues: Dict[str, Deque[Request]] = {m: deque() for m in models}
+        self.used = 0
+        self._blocked: Dict[int, float] = {}  # rid -> when it first did not fit
+
+    def submit(self, r: Request):
+        if self.footprint(r) > self.budget:
+            raise AdmissionRefused(f"request {r.rid} needs more than the whole budget")
+        self.queues.setdefault(r.model, deque()).append(r)
+
+    def cancel(self, rid: int) -> Optional[Request]:
+        """Remove a waiting request; None if no queue holds it."""
+        for q in self.queues.values():
+            for r in q:
+                if r.rid == rid:
+                    q.remove(r)
+                    self._blocked.pop(rid, None)
+                    return r
+        return None
+
+    def admit(self, now: float) -> List[Request]:
+        out: List[Request] = []
+        while True:
+            heads = sorted((q[0] for q in self.queues.values() if q and q[0].arrival <= now),
+                           key=lambda r: r.arrival)
+            took = False
+            for r in heads:
+                fp = self.footprint(r)
+                if self.used + fp <= self.budget:
+                    self.queues[r.model].popleft()
+                    self._blocked.pop(r.rid, None)
+                    self.used += fp
+                    out.append(r)
+                    took = True
+                    break  # the heads change: look again, oldest first
+                if now - self._blocked.setdefault(r.rid, now) >= self.max_bypass_s:
+                    return out  # it has waited long enough: nothing younger goes ahead of it
+            if not took:
+                return out
+
+    def release(self, r: Request):
+        self.used -= self.footprint(r)
+
+    def waiting(self) -> int:
+        return sum(len(q) for q in self.queues.values())
+
+
 class Server:
     def __init__(self, models=("d2q9", "d3q19"), precision="fp32", storage="same", budget_bytes: int = 150 << 30,
                  launch: Optional[Dict[str, Tuple[int, int, int]]] = None, max_cases: int = 4096,
-                 high_priority: Tuple[str, ...] = ("d2q9",)):
+                 high_priority: Tuple[str, ...] = ("d2q9",), max_bypass_s: float = 5.0):
         self.precision, self.storage = precision, storage
         self.budget = int(budget_bytes)
         self.batches: Dict[str, Batch] = {}
@@ -63,13 +132,17 @@ class Server:
             if m in high_priority:  # small cases: their blocks go first
                 b.set_priority(True)
             self.batches[m] = b
-        self.queue: Deque[Request] = deque()
+        self.adm = Admission(self.budget, self.footprint, models, max_bypass_s)
+        self.pending: Dict[str, List[Request]] = {m: [] for m in models}  # admitted, joining at the next boundary
         self.resident: Dict[Tuple[str, int], Request] = {}
-        self.used = 0
         self.done: List[Request] = []
+        self.cancelled: List[Request] = []
+        self._cancel_resident: set = set()
         self.t0 = time.perf_counter()
         self.rounds = 0
         self.busy = 0.0  # seconds with GPU work in flight (step to sync)
+        self.busy_by_model: Dict[str, float] = {m: 0.0 for m in models}  # seconds each model's batch was in flight
+        self.busy_all = 0.0  # seconds every model's batch was in flight at once
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -78,31 +151,64 @@ class Server:
         nz, ny, nx = r.spec.shape
         return case_bytes(r.model, nx, ny, nz, self.precision, self.storage)
 
-    def submit(self, r: Request):
-        if self.footprint(r) > self.budget:
-            raise AdmissionRefused(f"request {r.rid} needs more than the whole budget")
-        self.queue.append(r)
+    @property
+    def used(self) -> int:
+        return self.adm.used
 
-    def _admit(self, idle):
-        """Admit waiting requests in arrival order into idle batches while the
-        budget allows (first come, first served: the head of the queue waits
-        for memory, or for its batch's replay in flight)."""
-        now = self.now()
-        while self.queue and self.queue[0].arrival <= now:
-            r = self.queue[0]
-            fp = self.footprint(r)
-            if self.used + fp > self.budget or not idle[r.model]:
-                break
-            cid = self.batches[r.model].add_case(r.spec)
-            self.queue.popleft()
-            self.used += fp
+    def submit(self, r: Request):
+        self.adm.submit(r)
+
+    def cancel(self, rid: int) -> bool:
+        """Cancel a request: a waiting or pending one leaves at once, a running one at its batch's next
+        boundary. False if the request is unknown, finished or already cancelled."""
+        r = self.adm.cancel(rid)
+        if r is not None:
+            self._mark_cancelled(r, release=False)
+            return True
+        for m, lst in self.pending.items():
+            for r in lst:
+                if r.rid == rid:
+                    lst.remove(r)
+                    self._mark_cancelled(r)
+                    return True
+        for (m, cid), r in self.resident.items():
+            if r.rid == rid and not r.cancelled:
+                self._cancel_resident.add((m, cid))
+                return True
+        return False
+
+    def _mark_cancelled(self, r: Request, release: bool = True):
+        if release:
+            self.adm.release(r)
+        r.cancelled = True
+        r.finished = self.now()
+        self.cancelled.append(r)
+
+    def _admit(self):
+        """Admit what has arrived and fits (per-model queues, see Admission); admitted requests wait in their
+        model's pending list for the batch's next replay boundary."""
+        for r in self.adm.admit(self.now()):
             r.admitted = self.now()
-            self.resident[(r.model, cid)] = r
+            self.pending[r.model].append(r)
+
+    def _join(self, model):
+        """At a replay boundary of the model's batch: its pending cases join."""
+        b = self.batches[model]
+        for r in self.pending[model]:
+            cid = b.add_case(r.spec)
+            self.resident[(model, cid)] = r
+        self.pending[model] = []
 
     def _retire(self, model):
         b = self.batches[model]
         for (m, cid), r in list(self.resident.items()):
             if m != model:
+                continue
+            if (m, cid) in self._cancel_resident:
+                self._cancel_resident.discard((m, cid))
+                b.remove_case(cid)
+                del self.resident[(m, cid)]
+                self._mark_cancelled(r)
                 continue
             _done, rem = b.poll(cid)
             if rem > 0:
@@ -111,19 +217,25 @@ class Server:
             if r.want_quantity:
                 r.quantity = b.quantity(cid, r.want_quantity)
             b.remove_case(cid)
-            self.used -= self.footprint(r)
+            self.adm.release(r)
             r.finished = self.now()
             del self.resident[(m, cid)]
             self.done.append(r)
 
-    def run(self, requests: List[Request], timeout_s: float = 600.0) -> dict:
+    def run(self, requests: List[Request], timeout_s: float = 600.0,
+            cancels: Sequence[Tuple[float, int]] = ()) -> dict:
+        """Serve `requests` (arrival times relative to the start); `cancels` are (time, request id) events."""
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
+        cancel_events = sorted(cancels)
         self.t0 = time.perf_counter()
         inflight = {m: False for m in self.batches}
         t_prev = time.perf_counter()
-        while (self.queue or self.resident) and self.now() < timeout_s:
+        while (self.adm.waiting() or any(self.pending.values()) or self.resident) and self.now() < timeout_s:
             progressed = False
+            while cancel_events and cancel_events[0][0] <= self.now():
+                self.cancel(cancel_events.pop(0)[1])
+            self._admit()
             for m, b in self.batches.items():
                 if inflight[m]:
                     if not b.done():
@@ -132,10 +244,10 @@ class Server:
                     inflight[m] = False
                     self._retire(m)
                     progressed = True
-            idle = {m: not f for m, f in inflight.items()}
-            self._admit(idle)
-            for m, b in self.batches.items():
-                if not inflight[m] and b.pending_updates() > 0:
+                if self.pending[m] or self._cancel_resident:
+                    self._retire(m)  # cancelled cases leave before new ones join
+                    self._join(m)
+                if b.pending_updates() > 0:
                     b.step()
                     inflight[m] = True
                     self.rounds += 1
@@ -143,10 +255,16 @@ class Server:
             t = time.perf_counter()
             if any(inflight.values()):
                 self.busy += t - t_prev  # GPU work was in flight during this interval
+                for m, f in inflight.items():
+                    if f:
+                        self.busy_by_model[m] += t - t_prev
+                if all(inflight.values()):
+                    self.busy_all += t - t_prev
             t_prev = t
             if not progressed:
-                if not any(inflight.values()) and self.queue:
-                    dt = self.queue[0].arrival - self.now()
+                if not any(inflight.values()):
+                    nxt = [q[0].arrival for q in self.adm.queues.values() if q]
+                    dt = (min(nxt) - self.now()) if nxt else 0.0
                     if dt > 0:
                         time.sleep(min(dt, 0.005))
                         t_prev = time.perf_counter()
@@ -161,8 +279,10 @@ class Server:
         return {"requests": len(self.done), "wall_s": wall, "cases_per_s": len(self.done) / wall if wall else 0,
                 "mlups": upd / wall / 1e6 if wall else 0, "busy_s": self.busy,
                 "busy_mlups": upd / self.busy / 1e6 if self.busy else 0, "p50_s": float(np.percentile(tts, 50)),
-                "p99_s": float(np.percentile(tts, 99)), "rounds": self.rounds, "pending": len(self.queue) +
-                len(self.resident)}
+                "p99_s": float(np.percentile(tts, 99)), "rounds": self.rounds, "cancelled": len(self.cancelled),
+                "busy_by_model_s": dict(self.busy_by_model), "busy_all_models_s": self.busy_all,
+                "updates_by_model": {m: sum(r.updates for r in self.done if r.model == m) for m in self.batches},
+                "pending": self.adm.waiting() + sum(len(v) for v in self.pending.values()) + len(self.resident)}
 
     def close(self):
         for b in self.batches.values():

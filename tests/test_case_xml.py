@@ -606,8 +606,10 @@ def test_failcheck_stops_and_runs_final_actions(tmp_path):
     """<Failcheck> over the whole lattice (nx, ny given, as TCLB's examples do):
     a negative viscosity makes the run overflow to NaN (plain IEEE arithmetic);
     the check stops the Solve at its first failing call and runs its child
-    <VTK> there first. A Failcheck with a what= list naming no quantity checks
-    nothing and never stops the run."""
+    <VTK> there first. A child with its own Iterations= is not registered as a
+    periodic callback: it runs once, at the failing check, as TCLB's
+    Handler::DoIt runs each child once. A Failcheck with a what= list naming no
+    quantity checks nothing and never stops the run."""
     import subprocess
 
     runner = os.path.join(os.path.dirname(HERE), "tclb_b200", "tclb_run")
@@ -615,6 +617,8 @@ def test_failcheck_stops_and_runs_final_actions(tmp_path):
         '<Param name="Viscosity" value="0.02"/>', '<Param name="Viscosity" value="-0.2"/>')
     start, end = base.index("<Log "), base.index("</CLBConfig>")
     for name, fc, stops in (("whole", '<Failcheck Iterations="10" nx="256" ny="64"><VTK what="Rho"/></Failcheck>', True),
+                            ("child_iters", '<Failcheck Iterations="10" nx="256" ny="64"><VTK Iterations="5" '
+                                            'what="Rho"/></Failcheck>', True),
                             ("none", '<Failcheck Iterations="10" nx="256" ny="64" what="NoSuch"/>', False)):
         text = base[:start] + f'<Solve Iterations="300">{fc}<BIN Iterations="300"/></Solve>' + base[end:]
         path = tmp_path / f"{name}.xml"

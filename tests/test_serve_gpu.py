@@ -48,3 +48,34 @@ def test_results_same_alone_and_in_the_mix():
         alone.close()
         assert rel_l2(r.quantity, r2.quantity) <= 1e-6
         assert np.allclose(r.globals, r2.globals, rtol=1e-9, atol=1e-15)
+
+
+def test_cancel_waiting_pending_and_running_requests():
+    """A request cancelled while it waits for memory never runs; one cancelled
+    while it runs leaves at its batch's next boundary; the others finish with
+    the same results as without the cancellations, and all memory is returned."""
+    launch = {"d2q9": (64, 4, 16), "d3q19": (32, 8, 8)}
+    reqs = small_requests()
+    r1 = reqs[1]  # long enough to be running when it is cancelled at t = 0.06 s (it arrives at 0.01 s)
+    r1.spec = CaseSpec(r1.spec.flags, r1.spec.settings, r1.spec.zone_settings, 200000)
+    fps = [case_bytes(r.model, *r.spec.shape[::-1]) for r in reqs]
+    budget = max(fps) + sorted(fps)[-2]
+    srv = Server(("d2q9", "d3q19"), "fp32", "same", budget_bytes=budget, launch=launch)
+    # request 7 is cancelled before it arrives (still queued), request 1 while it runs
+    rep = srv.run(reqs, cancels=[(0.0, 7), (0.06, 1)])
+    srv.close()
+    by_id = {r.rid: r for r in reqs}
+    assert rep["pending"] == 0 and srv.used == 0
+    assert rep["requests"] + rep["cancelled"] == len(reqs)
+    assert by_id[7].cancelled and by_id[7].globals is None
+    assert by_id[1].cancelled and by_id[1].globals is None
+    for r in reqs:
+        if not r.cancelled:
+            assert r.globals is not None and r.quantity is not None
+    # an uncancelled request gives the same result as when served alone
+    r = by_id[2]
+    alone = Server((r.model,), "fp32", "same", budget_bytes=1 << 30, launch=launch)
+    r2 = Request(r.rid, r.model, r.spec, 0.0, want_quantity="U")
+    alone.run([r2])
+    alone.close()
+    assert rel_l2(r.quantity, r2.quantity) <= 1e-6

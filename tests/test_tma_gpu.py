@@ -33,11 +33,12 @@ PARAMS = {
 # (nz, ny, nx): rows per tile = 512 / nx; ny a multiple of it. Small ny makes
 # most tiles wrap at a y face (the one-row copies), larger ny has inner tiles.
 # nx = 192 gives 2-row tiles of 384 nodes: fewer than the 512 of the stage
-# layout, six consumer warps.
+# layout, six consumer warps. Rows wider than 256 (320 ... 512) are one-row
+# tiles copied with the split-x tensor maps (a (64, nx/64) box per row).
 SHAPES = {
-    "d2q9": [(1, 16, 128), (1, 8, 64), (1, 6, 256), (1, 8, 192)],
-    "d3q19": [(4, 8, 64), (3, 12, 128), (3, 6, 256), (3, 6, 192)],
-    "d3q27_cumulant": [(4, 8, 64), (3, 12, 128), (2, 6, 256), (2, 8, 192)],
+    "d2q9": [(1, 16, 128), (1, 8, 64), (1, 6, 256), (1, 8, 192), (1, 5, 384), (1, 3, 512), (1, 4, 448)],
+    "d3q19": [(4, 8, 64), (3, 12, 128), (3, 6, 256), (3, 6, 192), (2, 3, 384), (2, 2, 512), (1, 4, 320)],
+    "d3q27_cumulant": [(4, 8, 64), (3, 12, 128), (2, 6, 256), (2, 8, 192), (2, 3, 384), (1, 2, 512)],
 }
 
 
@@ -84,14 +85,14 @@ def test_tile_staged_matches_register_pairs_bit_for_bit(model, storage):
 
 
 def test_tile_staged_only_where_it_applies():
-    # FP32 storage, nx not a multiple of 64, nx above 256, ny not a multiple of 512/nx: no TMA
-    for args in [("d3q19", 64, 8, 2, "same"), ("d3q19", 96, 8, 2, "fp16s"), ("d3q19", 384, 4, 2, "fp16s"),
+    # FP32 storage, nx not a multiple of 64, nx above 512, ny not a multiple of 512/nx: no TMA
+    for args in [("d3q19", 64, 8, 2, "same"), ("d3q19", 96, 8, 2, "fp16s"), ("d3q19", 576, 4, 2, "fp16s"),
                  ("d3q19", 128, 6, 2, "fp16s")]:
         model, nx, ny, nz, st = args
         g = Lattice(model, nx, ny, nz, precision="fp32", storage=st)
         assert not g.launch_path()["tma"], args
         g.close()
-    for nx, ny in [(256, 4), (64, 8)]:
+    for nx, ny in [(256, 4), (64, 8), (384, 3), (512, 2)]:
         g = Lattice("d3q27_cumulant", nx, ny, 2, precision="fp32", storage="fp16s")
         assert g.launch_path()["tma"], nx
         g.close()
