@@ -257,12 +257,8 @@ struct Launch {
       const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
       const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
-      // the largest shared-memory carveout: blocks of narrow tiles (224 threads) then fit three per SM
-      // where their registers allow (d3q19), instead of the two the default carveout holds
       if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
               cudaSuccess ||
-          cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
           cudaFuncSetAttribute(k_iterate_tma<M, R, St, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_iterate_tma<M, R, St>, threads, smem) !=
