@@ -185,9 +185,9 @@ int tclb_sync(tclb_h h);
    accesses, and for d3q19 / d3q27_cumulant bulk nodes one packed FP32x2
    collision for both (on by default); TCLB_LAUNCH_TMA lets 16-bit storage
    stage tiles of whole rows in shared memory with TMA on plain iterations
-   (on by default; it takes precedence over PAIRS) when nx is a multiple of 64
-   up to 512 and ny a multiple of floor(512/nx). bx, by shape the one-node
-   kernel.
+   (on by default; it takes precedence over PAIRS) when nx is a multiple of 32
+   up to 512 (tiles of whole rows, at most 512 nodes, the number of rows
+   dividing ny). bx, by shape the one-node kernel.
    A staging wait that runs out (about a second) is reported as TCLB_ERR_CUDA
    by the next tclb_sync or Globals-reading tclb_iterate. */
 #define TCLB_LAUNCH_GRAPHS 1
@@ -276,8 +276,8 @@ int tclb_batch_get_launch(tclb_batch_h b, int* bx, int* by, int* iters_per_launc
    (blocks of bx / 2 x min(by, T / (bx / 2)) threads, T = 256, 128 for
    d3q27_cumulant); the Globals launch keeps the one-node kernel.
    TCLB_LAUNCH_TMA (on by default) runs the plain launches of each 16-bit case
-   whose rows fit one TMA box (nx a multiple of 64 up to 512, floor(512 / nx)
-   dividing ny) through the tile-staged kernel, tensor maps kept with the case;
+   whose rows fit the tile-staged kernel (nx a multiple of 32 up to 512) through
+   it, tensor maps kept with the case;
    the other cases take the pair or one-node form. A staging wait that runs
    out (about a second) is reported as TCLB_ERR_CUDA by the next
    tclb_batch_sync. TCLB_BATCH_ADAPTIVE (on by default) fits the launches to

@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       }
       if (lane == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(Rr * nx) * 2u);
+        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(Rr * tma_pitch(nx)) * 2u);
       }
       __syncwarp();
       tma_fill_at<M>(&mp->rows[parity], &mp->row1[parity], &mp->flags, stages + s * stage_elems, fb, tile.z,
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       ny = C.ny;
       const int half = nx >> 1;
       r = tid / half;
-      x = 2 * (tid % half);  // whole warps per row (nx a multiple of 64)
+      x = 2 * (tid % half);  // a warp may span two rows (nx a multiple of 32)
       act = r < C.tma_rows;
       xm = x == 0 ? nx - 1 : x - 1;
       xp2 = x + 2 == nx ? 0 : x + 2;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
     float2 v[M::Q];
     unsigned fl2 = 0;
     if (act) {
-      const unsigned short* mine = stages + s * stage_elems + r * nx;  // this thread's row, population 0
+      const unsigned short* mine = stages + s * stage_elems + r * tma_pitch(nx);  // this thread's row, population 0
 #pragma unroll
       for (int i = 0; i < M::Q; i++) {
         const unsigned short* row = mine + i * block;

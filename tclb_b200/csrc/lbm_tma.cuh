@@ -38,19 +38,29 @@ struct TmaMaps {
   CUtensorMap flags;  // node types: dims (nx, ny, nz), box (nx, R, 1)
 };
 
-// Rows per tile of a lattice for the tile-staged kernels: 16-bit storage, nx
-// a multiple of 64 up to 512, R = floor(512 / nx) rows dividing ny; 0 where
-// they do not apply. A row is one TMA box: up to 256 values as one box row
-// (TMA boxes are at most 256 values along a dimension), wider rows as a
-// (64, nx/64) box of a tensor whose x axis is split in two (64 x nx/64), which
-// lands in shared memory in the same row-major order.
+// Tiles of the tile-staged kernels: 16-bit storage, nx a multiple of 32
+// (TCLB pads nx so) up to 512. A row is one TMA box: up to 256 values as one
+// box row (TMA boxes are at most 256 values along a dimension), wider rows as
+// a (32, nx/32) box of a tensor whose x axis is split in two (32 x nx/32),
+// which lands in shared memory in the same row-major order. In shared memory
+// the rows of a tile lie `pitch` values apart: nx rounded up to a multiple of
+// 64 for rows of at most 256 (the box is that wide; the values past nx are
+// the copy's out-of-range zero fill), so that every row a TMA copy writes
+// starts on a 128-byte boundary; rows wider than 256 come one per tile.
+// R, the rows per tile, is the largest count with R * pitch <= 512 that
+// divides ny; 0 where the kernel does not apply.
 constexpr int TMA_MAX_NX = 512;
-inline int tma_rows_for(size_t elem, int nx, int ny) {
-  if (elem != 2 || nx % 64 || nx > TMA_MAX_NX) return 0;
-  const int R = 512 / nx;
-  return ny % R ? 0 : R;
-}
 __host__ __device__ inline bool tma_wide(int nx) { return nx > 256; }
+__host__ __device__ inline int tma_pitch(int nx) { return tma_wide(nx) ? nx : (nx + 63) / 64 * 64; }
+inline int tma_rows_for(size_t elem, int nx, int ny) {
+  if (elem != 2 || nx < 32 || nx % 32 || nx > TMA_MAX_NX) return 0;
+  for (int R = 512 / tma_pitch(nx); R >= 1; R--)
+    if (ny % R == 0) return R;
+  return 0;
+}
+// Threads of a tile-staged block: the tile's node pairs, rounded up to whole
+// warps, and one producer warp.
+inline int tma_threads(int R, int nx) { return ((R * nx / 2 + 31) / 32 + 1) * 32; }  // R * nx / 2 pairs
 
 // The driver's cuTensorMapEncodeTiled, reached through the runtime's
 // entry-point query so the library links only the runtime; null if absent.
@@ -81,12 +91,12 @@ inline bool encode_tile_maps(void* buf, const void* flags, int nx, int ny, int n
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return false;
   const cuuint64_t e = 2;
-  if (tma_wide(nx)) {  // x split as (64, nx/64): rows (64, nx/64, ny, nz, Q), node types (64, nx/64, ny, nz)
-    const cuuint32_t xo = (cuuint32_t)(nx / 64);
-    const cuuint64_t dims[5] = {64, xo, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
-    const cuuint64_t strides[4] = {64 * e, nx * e, (cuuint64_t)nx * ny * e, stride * e};
-    const cuuint32_t box_rows[5] = {64, xo, (cuuint32_t)R, 1, 1};
-    const cuuint32_t box_row1[5] = {64, xo, 1, 1, 1};
+  if (tma_wide(nx)) {  // x split as (32, nx/32): rows (32, nx/32, ny, nz, Q), node types (32, nx/32, ny, nz)
+    const cuuint32_t xo = (cuuint32_t)(nx / 32);
+    const cuuint64_t dims[5] = {32, xo, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
+    const cuuint64_t strides[4] = {32 * e, nx * e, (cuuint64_t)nx * ny * e, stride * e};
+    const cuuint32_t box_rows[5] = {32, xo, (cuuint32_t)R, 1, 1};
+    const cuuint32_t box_row1[5] = {32, xo, 1, 1, 1};
     const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
     if (enc(rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 5, buf, dims, strides, box_rows, ones,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -96,17 +106,18 @@ inline bool encode_tile_maps(void* buf, const void* flags, int nx, int ny, int n
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
-    const cuuint64_t fdims[4] = {64, xo, (cuuint64_t)ny, (cuuint64_t)nz};
-    const cuuint64_t fstrides[3] = {64 * e, nx * e, (cuuint64_t)nx * ny * e};
-    const cuuint32_t fbox[4] = {64, xo, (cuuint32_t)R, 1};
+    const cuuint64_t fdims[4] = {32, xo, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t fstrides[3] = {32 * e, nx * e, (cuuint64_t)nx * ny * e};
+    const cuuint32_t fbox[4] = {32, xo, (cuuint32_t)R, 1};
     return enc(fmap, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, const_cast<void*>(flags), fdims, fstrides, fbox, ones,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   }
+  const cuuint32_t pitch = (cuuint32_t)tma_pitch(nx);  // box width: nx rounded up to 64, zero-filled past nx
   const cuuint64_t dims[4] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)Q};
   const cuuint64_t strides[3] = {nx * e, (cuuint64_t)nx * ny * e, stride * e};
-  const cuuint32_t box_rows[4] = {(cuuint32_t)nx, (cuuint32_t)R, 1, 1};
-  const cuuint32_t box_row1[4] = {(cuuint32_t)nx, 1, 1, 1};
+  const cuuint32_t box_rows[4] = {pitch, (cuuint32_t)R, 1, 1};
+  const cuuint32_t box_row1[4] = {pitch, 1, 1, 1};
   const cuuint32_t ones[4] = {1, 1, 1, 1};
   if (enc(rows, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, buf, dims, strides, box_rows, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -118,7 +129,7 @@ inline bool encode_tile_maps(void* buf, const void* flags, int nx, int ny, int n
     return false;
   const cuuint64_t fdims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
   const cuuint64_t fstrides[2] = {nx * e, (cuuint64_t)nx * ny * e};
-  const cuuint32_t fbox[3] = {(cuuint32_t)nx, (cuuint32_t)R, 1};
+  const cuuint32_t fbox[3] = {pitch, (cuuint32_t)R, 1};
   return enc(fmap, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(flags), fdims, fstrides, fbox, ones,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -239,7 +250,7 @@ __device__ __forceinline__ void tma_fill_at(const CUtensorMap* rows, const CUten
         int y = ys + r;
         y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
         if (wide) tma_load_5d(dst + (unsigned)(r * nx * 2), row1, 0, 0, y, zs, i, bar);
-        else tma_load_4d(dst + (unsigned)(r * nx * 2), row1, 0, y, zs, i, bar);
+        else tma_load_4d(dst + (unsigned)(r * tma_pitch(nx) * 2), row1, 0, y, zs, i, bar);
       }
     }
   } else if (lane == M::Q) {
@@ -257,8 +268,9 @@ __device__ __forceinline__ void tma_fill(const TmaMaps& T, unsigned short* stage
   tma_fill_at<M>(&T.rows, &T.row1, &T.flags, stage, bar, z, y0, nx, ny, nz, R, lane);
 }
 
-// The kernel: ncons = R*nx/64 = TMA_CONSUMERS warps update node pairs, one
-// more warp (the last) produces. Block = (ncons + 1) * 32 threads; the
+// The kernel: ncons = ceil(R*nx/64) <= TMA_CONSUMERS warps update node
+// pairs (threads past the tile's R*nx/2 pairs only take part in the stage
+// protocol), one more warp (the last) produces. Block = (ncons + 1) * 32 threads; the
 // consumer warps cover the tile's R*nx/2 pairs, one pair per thread. Grid = resident blocks
 // (persistent), walking tiles t = blockIdx.x + k*gridDim.x.
 // Dynamic shared memory: 128 bytes of mbarriers (full[S], empty[S]), then
@@ -284,8 +296,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   static_assert(TMA_STAGES <= 8, "128 bytes hold 8 full and 8 empty barriers");
   unsigned long long* empty = full + 8;
   unsigned short* stages = reinterpret_cast<unsigned short*>(smem + 128);
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  constexpr unsigned block = TMA_TILE;  // R_rows * nx: a compile-time stride for the stage layout
+  const int nx = a.nx, ny = a.ny, nz = a.nz, pitch = tma_pitch(nx);
+  constexpr unsigned block = TMA_TILE;  // R_rows * pitch at most: a compile-time stride for the stage layout
   constexpr unsigned stage_elems = (M::Q + 1) * block;
   const int ntiles = nz * (ny / R_rows);
   const int rows_per_plane = ny / R_rows;
@@ -320,7 +332,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       }
       if (lane == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(R_rows * nx) * 2u);  // the bytes of R_rows rows
+        mbar_expect_tx(fb, (unsigned)(M::Q + 1) * (unsigned)(R_rows * pitch) * 2u);  // R_rows boxed rows
       }
       __syncwarp();
       if (!FAULT || t != skip_tile) tma_fill<M>(T, stages + s * stage_elems, fb, t, nx, ny, nz, R_rows, lane);
@@ -330,7 +342,9 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
 
   // consumers
   const int half = nx >> 1;
-  const int r = tid / half, x = 2 * (tid % half);  // whole warps per row (nx >= 64)
+  const int r = tid / half, x = 2 * (tid % half);  // a warp may span two rows (nx a multiple of 32)
+  const bool act = r < R_rows;                     // threads past the tile's pairs
+
   const int xm = x == 0 ? nx - 1 : x - 1, xp2 = x + 2 == nx ? 0 : x + 2;
   // tile t = (z, yt) with yt = t mod rows_per_plane, stepped by gridDim.x per
   // round without a division; the stage index and its phase likewise
@@ -345,21 +359,24 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       return;
     }
     const unsigned short* st = stages + s * stage_elems;
-    const unsigned short* mine = st + r * nx;  // this thread's row in population block 0
+    const unsigned short* mine = st + r * pitch;  // this thread's row in population block 0
     const int y = yt * R_rows + r;
     float2 v[M::Q];
+    unsigned fl2 = 0;
+    if (act) {
 #pragma unroll
-    for (int i = 0; i < M::Q; i++) {
-      const unsigned short* row = mine + i * block;  // constant offset per population
-      if (M::ex(i) == 0) {
-        v[i] = P16::unpack(*reinterpret_cast<const unsigned*>(row + x));
-      } else if (M::ex(i) > 0) {  // from x-1
-        v[i] = make_float2(P16::lo(row[xm]), P16::lo(row[x]));
-      } else {  // from x+1
-        v[i] = make_float2(P16::lo(row[x + 1]), P16::lo(row[xp2]));
+      for (int i = 0; i < M::Q; i++) {
+        const unsigned short* row = mine + i * block;  // constant offset per population
+        if (M::ex(i) == 0) {
+          v[i] = P16::unpack(*reinterpret_cast<const unsigned*>(row + x));
+        } else if (M::ex(i) > 0) {  // from x-1
+          v[i] = make_float2(P16::lo(row[xm]), P16::lo(row[x]));
+        } else {  // from x+1
+          v[i] = make_float2(P16::lo(row[x + 1]), P16::lo(row[xp2]));
+        }
       }
+      fl2 = *reinterpret_cast<const unsigned*>(mine + M::Q * block + x);
     }
-    const unsigned fl2 = *reinterpret_cast<const unsigned*>(mine + M::Q * block + x);
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&empty[s]));  // this warp is done with the stage
     const unsigned node = (unsigned)x + (unsigned)nx * ((unsigned)y + (unsigned)ny * (unsigned)z);
@@ -373,7 +390,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       yt -= rows_per_plane;
       z++;
     }
-    pair_update_store<M, R, St>(v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
+    if (act) pair_update_store<M, R, St>(v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
   }
 }
 

@@ -222,7 +222,7 @@ struct Launch {
         P.d[i] = static_cast<T*>(dst) + (size_t)i * L->stride;
       }
       if (L->use_tma && L->tma_ok && !glob) {  // tiles staged in shared memory by TMA
-        const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
+        const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
         const size_t smem = tma_smem_bytes<M>();
         if (L->tma_grid > 0) {
           if (L->fault_tile >= 0 || L->wait_cycles != TMA_WAIT_CYCLES)  // the failure-path test
@@ -254,7 +254,7 @@ struct Launch {
     using T = typename St::T;
     if constexpr (sizeof(T) == 2) {
       if (!L->tma_ok) return;
-      const int rows = L->tma_rows, threads = (rows * L->nx / 64 + 1) * 32;
+      const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
       const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
       if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -332,9 +332,9 @@ const Impl* impl_for(int model, int precision, int storage) {
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Tensor maps of the tile-staged kernel (16-bit storage, nx a multiple of 64
-// and at most 512, R = floor(512 / nx) rows per tile dividing ny). When
-// anything does not fit, tma_ok stays 0 and the register kernels run.
+// Tensor maps of the tile-staged kernel (16-bit storage, nx a multiple of 32
+// and at most 512, R <= 512 / nx rows per tile dividing ny). When anything
+// does not fit, tma_ok stays 0 and the register kernels run.
 void setup_tma(tclb_lattice* L) {
   L->tma_ok = 0;
   // Tiles of at most 512 nodes (R whole rows; one row when nx > 256, copied

@@ -214,9 +214,13 @@ def test_reduced_storage_d3q19(storage):
     run_both(g, o, 200, M.ITER_NORM)
     err = rel_l2(g.GetQuantity("U"), o.quantity("U"))
     print(f"{storage}: velocity rel L2 against the FP64 oracle {err:.3e}")
-    # unshifted 16-bit storage cannot hold the ~1e-3 velocity signal on top of
-    # f ~ w_i (half: 11-bit mantissa); the shifted formats store f - w_i.
-    bound = {"fp16s": 1e-2, "bf16s": 1e-1, "fp16": 1.5, "bf16": 2.0}[storage]
+    # Measured on B200: fp16s 2.9e-4, bf16s 3.0e-3, fp16 1.9e-2, bf16 1.0. The
+    # shifted FP16 format meets the 1e-3 bar on this flow; the bars below are
+    # about 3x the measured errors. Unshifted 16-bit storage cannot hold the
+    # ~1e-3 velocity signal on top of f ~ w_i (BF16 loses it entirely: its
+    # spacing at w_i is above the per-step increments); the shifted formats
+    # store f - w_i.
+    bound = {"fp16s": 1e-3, "bf16s": 1e-2, "fp16": 6e-2, "bf16": 2.0}[storage]
     assert err < bound, f"{storage}: velocity rel L2 {err:.3e}"
 
 
