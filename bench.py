@@ -72,7 +72,8 @@ def parse():
     p.add_argument("--rate", type=float, default=6.0, help="config 5: Poisson arrival rate (requests/s)")
     p.add_argument("--path", default="auto", choices=["auto", "tma", "pairs", "one"],
                    help="16-bit storage kernel for plain iterations: auto (tile-staged TMA where it "
-                        "applies, else two nodes per thread), tma, pairs, one (one node per thread)")
+                        "applies and is the faster choice, else two nodes per thread), tma, pairs, one "
+                        "(one node per thread)")
     p.add_argument("--case", default="tgv", choices=["tgv", "porous"],
                    help="timed lattice: the Taylor-Green vortex (the headline) or, with --shape, the d3q19 porous "
                         "channel of configuration 3 (Bernoulli(0.08) solids, ForceX 1e-6, nu 0.01) for profiling")
@@ -401,7 +402,8 @@ def run_ours(args):
     lat = case_lattice(args)
     if args.path != "auto":
         lat.set_launch(128 if lat.nx >= 128 else 32, 2 if lat.nx >= 128 else 8, use_graphs=True,
-                       use_pairs=args.path in ("pairs", "tma"), use_tma=args.path == "tma")
+                       use_pairs=args.path in ("pairs", "tma"), use_tma=args.path == "tma",
+                       tma_always=args.path == "tma")
     path = lat.launch_path()
     # a dedicated (non-default) stream: the library launches on it, the CUDA
     # events below are recorded on it

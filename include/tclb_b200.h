@@ -193,6 +193,10 @@ int tclb_sync(tclb_h h);
 #define TCLB_LAUNCH_GRAPHS 1
 #define TCLB_LAUNCH_PAIRS 2
 #define TCLB_LAUNCH_TMA 4
+/* With TCLB_LAUNCH_TMA: stage tiles wherever the tile-staged kernel applies,
+   also for d3q19 rows wider than 256, which otherwise take the register pair
+   kernel (measured faster there). */
+#define TCLB_LAUNCH_TMA_ALWAYS 8
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);
 /* The launch shape and the paths plain iterations take on this lattice: the
    flags that are both enabled and applicable (no TCLB counterpart). */

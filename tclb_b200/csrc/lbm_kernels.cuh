@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "f32x2.cuh"
 #include "tclb_models.h"
@@ -112,6 +113,7 @@ struct D2Q9 {
   static constexpr int Q = 9, DIM = 2, NSET = d2q9::NSET, NZS = d2q9::NZS, NG = d2q9::NG, NSUM = d2q9::NSUM,
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
   static constexpr bool has_bulk = false;  // no packed two-node collision
+  static constexpr bool identity_lanes = false;
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 4;  // <= 64 registers
   static constexpr int BATCH_MIN_BLOCKS = 6;  // one-tile batch kernel: <= 40 registers
   __device__ __forceinline__ static bool collides(flag_t) { return false; }
@@ -422,8 +424,14 @@ struct D3Q19 {
   // deviations g = f - w: the sum of g is rho - 1, which enters the
   // equilibrium's terms linear in rho (giving feq - w), while the quadratic
   // terms and the force use the true density.
+  // `lanes` (two-node form only) gives per-lane rates and force: a lane whose
+  // node does not collide gets gamma1 = gamma2 = 1 and no force, which maps its
+  // values onto themselves up to FP32 rounding (far below the 16-bit storage
+  // the two-node form serves).
+  struct Lanes { F2 g1, g2, fx, fy, fz; };
   template <bool DEV = false, class V, class AR>
-  __device__ __forceinline__ static void trt(V (&f)[Q], const AR& a, V& rho, V& jx, V& jy, V& jz) {
+  __device__ __forceinline__ static void trt(V (&f)[Q], const AR& a, V& rho, V& jx, V& jy, V& jz,
+                                             const Lanes* lanes = nullptr) {
     V s[9], d[9];
 #pragma unroll
     for (int p = 0; p < 9; p++) {
@@ -434,14 +442,25 @@ struct D3Q19 {
     jx = d[0] + d[3] - d[4] + d[5] - d[6];
     jy = d[1] + d[3] + d[4] + d[7] - d[8];
     jz = d[2] + d[5] + d[6] + d[7] + d[8];
-    const V g1 = V(a.k[0]), g2 = V(a.k[1]);
+    V g1, g2, fx, fy, fz;
+    if constexpr (std::is_same<V, F2>::value) {
+      if (lanes) {
+        g1 = lanes->g1, g2 = lanes->g2, fx = lanes->fx, fy = lanes->fy, fz = lanes->fz;
+      } else {
+        g1 = V(a.k[0]), g2 = V(a.k[1]);
+        fx = V(a.s[d3q19::S_ForceX]), fy = V(a.s[d3q19::S_ForceY]), fz = V(a.s[d3q19::S_ForceZ]);
+      }
+    } else {
+      g1 = V(a.k[0]), g2 = V(a.k[1]);
+      fx = V(a.s[d3q19::S_ForceX]), fy = V(a.s[d3q19::S_ForceY]), fz = V(a.s[d3q19::S_ForceZ]);
+    }
     const V rho_t = DEV ? rho + V(1) : rho;  // true density
     const V irho = recip(rho_t);
     V e0, e[9], o[9];
     feq_parts<!DEV>(rho, irho, jx, jy, jz, e0, e, o);
-    jx += rho_t * V(a.s[d3q19::S_ForceX]);
-    jy += rho_t * V(a.s[d3q19::S_ForceY]);
-    jz += rho_t * V(a.s[d3q19::S_ForceZ]);
+    jx += rho_t * fx;
+    jy += rho_t * fy;
+    jz += rho_t * fz;
     V e0n, en[9], on[9];
     feq_parts<!DEV>(rho, irho, jx, jy, jz, e0n, en, on);
     f[0] = e0n + g1 * (f[0] - e0);
@@ -552,6 +571,21 @@ struct D3Q19 {
   __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const AR& a) {
     F2 rho, jx, jy, jz;
     trt<DEV>(f, a, rho, jx, jy, jz);
+  }
+  // A pair where one node collides and the other does not (fluid next to a
+  // wall or a solid): the other lane takes the identity rates, so no copy of
+  // it is kept across the collision. Rates and force are selected per lane
+  // for every pair (exact selects), so all pairs take the same path.
+  static constexpr bool identity_lanes = true;
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair_lanes(F2 (&f)[Q], bool ca, bool cb, const AR& a) {
+    F2 rho, jx, jy, jz;
+    const float g1 = (float)a.k[0], g2 = (float)a.k[1];
+    const float fx = (float)a.s[d3q19::S_ForceX], fy = (float)a.s[d3q19::S_ForceY], fz = (float)a.s[d3q19::S_ForceZ];
+    const Lanes L{F2(ca ? g1 : 1.0f, cb ? g1 : 1.0f), F2(ca ? g2 : 1.0f, cb ? g2 : 1.0f),
+                  F2(ca ? fx : 0.0f, cb ? fx : 0.0f), F2(ca ? fy : 0.0f, cb ? fy : 0.0f),
+                  F2(ca ? fz : 0.0f, cb ? fz : 0.0f)};
+    trt<DEV>(f, a, rho, jx, jy, jz, &L);
   }
 
   // SetEquilibrum (:212-217): f = Req(rho, J) . MRTMAT.inv
@@ -796,6 +830,9 @@ struct D3Q27C {
     m[24] += V(sign * (1.0f / 9.0f));
     m[26] += V(sign * (1.0f / 27.0f));
   }
+  static constexpr bool identity_lanes = false;  // orders above 3 are set to zero: no identity rates
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair_lanes(F2 (&)[Q], bool, bool, const AR&) {}
   template <bool DEV, class AR>
   __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t fla, flag_t flb, const AR& a) {
     typedef typename AR::real R;
@@ -1043,7 +1080,11 @@ struct Pack16<StoreBF16<SH>> {
 // iterations (no Globals).
 // AR: Args<R, M::NSET>, or for the packed models a view with the same
 // members s[], k[], zone (SharedArgsView).
-template <class M, class R, class St, class A, class AR>
+// LANES (register pair kernels of models with identity rates, d3q19): a pair
+// where one node collides runs the other lane at the identity rates instead
+// of parking it. The tile-staged kernels keep parking: their 96-register cap
+// (18 warps per SM) spills the per-lane rates, which cost more than parking.
+template <class M, class R, class St, class A, class AR, bool LANES = false>
 __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb, const AR& a, const A& P,
                                                   unsigned node) {
   using P16 = Pack16<St>;
@@ -1075,7 +1116,9 @@ __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla,
       for (int i = 0; i < M::Q; i++) f2[i].v.y = t[i] - SH * (float)M::w(i);
     }
     const bool ca = M::collides(fla), cb = M::collides(flb);
-    if (ca || cb) {
+    if constexpr (LANES && M::identity_lanes) {
+      if (ca || cb) M::template collide_pair_lanes<St::shifted>(f2, ca, cb, a);
+    } else if (ca || cb) {
       // A pair where only one node collides (fluid next to a wall) parks the
       // other node's values in thread-local memory across the collision; a
       // volatile array keeps them out of the registers every pair would pay.
@@ -1164,7 +1207,7 @@ __device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a, cons
       v[i] = make_float2(P16::hi(w), P16::lo(next));
     }
   }
-  if (!PARTIAL || store) pair_update_store<M, R, St>(v, fla, flb, a, P, node);
+  if (!PARTIAL || store) pair_update_store<M, R, St, A, Args<R, M::NSET>, true>(v, fla, flb, a, P, node);
 }
 
 // Block (32, M::PAIR_THREADS / 32): each warp covers 64 consecutive x of one

@@ -161,6 +161,9 @@ struct tclb_lattice {
   // 16-bit storage: tile-staged TMA kernel (tma_rows rows per tile; tma[b]
   // describes snapshot b as the source), and its error word in the pool
   int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_grid = 0;
+  // rows wider than 256 of a model whose register pair kernel measured faster
+  // there (d3q19): plain iterations take that kernel unless tma_always
+  int tma_pref_pairs = 0, tma_always = 0;
   TmaMaps tma[2];
   int* err_dev = nullptr;
   // failure-path test of the tile-staged kernel (tclb_set_fault_injection):
@@ -200,6 +203,12 @@ Args<R, M::NSET> make_args(const tclb_lattice* L, const void* src, void* dst) {
   return a;
 }
 
+// Plain iterations of 16-bit storage take the tile-staged kernel.
+inline bool tma_path(const tclb_lattice* L) {
+  return L->use_tma && L->tma_ok && L->tma_grid > 0 &&
+         (L->tma_always || !L->tma_pref_pairs || !(L->use_pairs && L->nx % 64 == 0));
+}
+
 inline dim3 grid_of(const tclb_lattice* L) {
   return dim3((L->nx + L->bx - 1) / L->bx, (L->ny + L->by - 1) / L->by, L->nz);
 }
@@ -221,7 +230,7 @@ struct Launch {
         P.s[i] = static_cast<const T*>(src) + (size_t)i * L->stride;
         P.d[i] = static_cast<T*>(dst) + (size_t)i * L->stride;
       }
-      if (L->use_tma && L->tma_ok && !glob) {  // tiles staged in shared memory by TMA
+      if (tma_path(L) && !glob) {  // tiles staged in shared memory by TMA
         const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
         const size_t smem = tma_smem_bytes<M>();
         if (L->tma_grid > 0) {
@@ -254,6 +263,10 @@ struct Launch {
     using T = typename St::T;
     if constexpr (sizeof(T) == 2) {
       if (!L->tma_ok) return;
+      // d3q19 with one-row tiles (nx > 256): six consumer warps per block, and the
+      // register pair kernel with identity-rate lanes measured faster (porous
+      // 384x192x192: 57.7k against 51.3k MLUPS); narrower rows stay staged
+      if constexpr (M::identity_lanes) L->tma_pref_pairs = tma_wide(L->nx) && L->nx % 64 == 0;
       const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
       const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
@@ -1029,6 +1042,7 @@ int tclb_set_launch(tclb_h L, int bx, int by, int flags) {
   L->use_graphs = (flags & TCLB_LAUNCH_GRAPHS) ? 1 : 0;
   L->use_pairs = (flags & TCLB_LAUNCH_PAIRS) ? 1 : 0;
   L->use_tma = (flags & TCLB_LAUNCH_TMA) ? 1 : 0;
+  L->tma_always = (flags & TCLB_LAUNCH_TMA_ALWAYS) ? 1 : 0;
   return TCLB_OK;
 }
 
@@ -1047,7 +1061,7 @@ int tclb_get_launch(tclb_h L, int* bx, int* by, int* flags) {
   if (bx) *bx = L->bx;
   if (by) *by = L->by;
   if (flags) {
-    const bool tma = L->use_tma && L->tma_ok && L->tma_grid > 0;
+    const bool tma = tma_path(L);
     const bool pairs = !tma && L->use_pairs && L->elem == 2 && L->nx % 64 == 0;
     *flags = (L->use_graphs ? TCLB_LAUNCH_GRAPHS : 0) | (pairs ? TCLB_LAUNCH_PAIRS : 0) | (tma ? TCLB_LAUNCH_TMA : 0);
   }

@@ -308,6 +308,7 @@ class Lattice:
         wait by wait_cycles clock cycles; the next sync() raises TCLBError. tile=-1, wait_cycles=0: off."""
         _check(self.lib.tclb_set_fault_injection(self._h, int(tile), int(wait_cycles)))
 
-    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True, use_tma: bool = True):
-        flags = (1 if use_graphs else 0) | (2 if use_pairs else 0) | (4 if use_tma else 0)
+    def set_launch(self, bx: int, by: int, use_graphs: bool = True, use_pairs: bool = True, use_tma: bool = True,
+                   tma_always: bool = False):
+        flags = (1 if use_graphs else 0) | (2 if use_pairs else 0) | (4 if use_tma else 0) | (8 if tma_always else 0)
         _check(self.lib.tclb_set_launch(self._h, int(bx), int(by), flags))

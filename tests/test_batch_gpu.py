@@ -274,10 +274,12 @@ TMA_SHAPES = {
 @pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
 @pytest.mark.parametrize("storage", ["fp16s", "bf16"])
 def test_batch_tile_staged_matches_pairs_bit_for_bit(model, storage):
-    """Cases whose rows fit one TMA box (nx 64, 128, 192, 256) take the
-    tile-staged batch kernel, the others (nx = 96) the pair kernel, in one
-    batch; every field and Globals vector must equal that of the same batch
-    with staging off (the same pair update on the same values)."""
+    """Cases whose rows fit the tile-staged kernel (nx a multiple of 32 up to
+    512: here 64, 96, 128, 192, 256) take the tile-staged batch kernel, a case
+    with other settings the pair kernel, in one batch; every field and Globals
+    vector must equal that of the same batch with staging off (the same pair
+    update on the same values; nx = 96 runs its last tile of each row
+    half-filled in the pair form)."""
     specs = [_random_case(model, sh, seed=41 + i, niter=9) for i, sh in enumerate(TMA_SHAPES[model])]
     # a case that fits the staged kernel but has other settings: for the
     # packed-collision models it leaves the staged group and takes the pairs

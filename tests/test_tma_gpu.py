@@ -52,7 +52,7 @@ SHAPES = {
 def run(model, shape, storage, fl, f0, tma, pairs, niter=5):
     m = M.get(model)
     g = Lattice(model, shape[2], shape[1], shape[0], precision="fp32", storage=storage)
-    g.set_launch(32, 8, use_graphs=True, use_pairs=pairs, use_tma=tma)
+    g.set_launch(32, 8, use_graphs=True, use_pairs=pairs, use_tma=tma, tma_always=tma)
     path = g.launch_path()
     g.set_flags(fl)
     apply_params(g, PARAMS[model])
