@@ -282,7 +282,9 @@ constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
 // producer arms tile skip_tile's stage but issues none of its copies, so its
 // consumers' wait runs out. Without FAULT both parameters are ignored and
 // the waits keep the compile-time bound.
-template <class M, class R, class St, bool FAULT = false>
+// PARTIAL: the tile's pairs do not fill whole warps (R * nx / 2 not a
+// multiple of 32), so consumer threads check that they hold a pair.
+template <class M, class R, class St, bool FAULT = false, bool PARTIAL = false>
 __global__ void __launch_bounds__(TMA_THREADS, 2)
     k_iterate_tma(const Args<R, M::NSET> a, const __grid_constant__ TmaMaps T,
                   const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err, long long wait_cycles_arg,
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   // consumers
   const int half = nx >> 1;
   const int r = tid / half, x = 2 * (tid % half);  // a warp may span two rows (nx a multiple of 32)
-  const bool act = r < R_rows;                     // threads past the tile's pairs
+  const bool act = !PARTIAL || r < R_rows;         // threads past the tile's pairs
 
   const int xm = x == 0 ? nx - 1 : x - 1, xp2 = x + 2 == nx ? 0 : x + 2;
   // tile t = (z, yt) with yt = t mod rows_per_plane, stepped by gridDim.x per

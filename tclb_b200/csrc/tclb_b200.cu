@@ -234,9 +234,13 @@ struct Launch {
         const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
         const size_t smem = tma_smem_bytes<M>();
         if (L->tma_grid > 0) {
+          const bool partial = (rows * L->nx / 2) % 32 != 0;  // pairs that do not fill whole warps
           if (L->fault_tile >= 0 || L->wait_cycles != TMA_WAIT_CYCLES)  // the failure-path test
-            k_iterate_tma<M, R, St, true><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev,
-                                                                            L->wait_cycles, L->fault_tile);
+            k_iterate_tma<M, R, St, true, true><<<L->tma_grid, threads, smem, s>>>(
+                a, L->tma[L->cur], P, rows, L->err_dev, L->wait_cycles, L->fault_tile);
+          else if (partial)
+            k_iterate_tma<M, R, St, false, true><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows,
+                                                                                   L->err_dev, TMA_WAIT_CYCLES, -1);
           else
             k_iterate_tma<M, R, St><<<L->tma_grid, threads, smem, s>>>(a, L->tma[L->cur], P, rows, L->err_dev,
                                                                         TMA_WAIT_CYCLES, -1);
@@ -272,7 +276,9 @@ struct Launch {
       int per_sm = 0, sms = 0;
       if (cudaFuncSetAttribute(k_iterate_tma<M, R, St>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
               cudaSuccess ||
-          cudaFuncSetAttribute(k_iterate_tma<M, R, St, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          cudaFuncSetAttribute(k_iterate_tma<M, R, St, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem) != cudaSuccess ||
+          cudaFuncSetAttribute(k_iterate_tma<M, R, St, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_iterate_tma<M, R, St>, threads, smem) !=
               cudaSuccess ||
