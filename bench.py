@@ -17,7 +17,9 @@ FP16-shift storage (the tile-staged kernel) and in FP64, each timed on the
 device like the headline (MLUPS, the iteration kernel's fraction of the
 measured HBM bandwidth, the ratio to the FP32 line), and each storage's
 relative L2 velocity error against the FP64 run after 2000 iterations from the
-same initial state.
+same initial state. It also carries ``other_configs``: configuration 3 (the
+d3q19 porous channel in four storages, with their errors against FP64) and
+configuration 4 (512 batched d2q9 cases, FP32 and FP16-shift).
 
 Multi-GPU (torchrun, one rank per GPU): independent replicas, weak scaling, no
 data-path collective (the case does not shard across GPUs here).
@@ -67,6 +69,8 @@ def parse():
                    help="N=1: storage variants timed after the headline on the same workload "
                         "(comma list of fp16s, bf16s, fp64; empty for none)")
     p.add_argument("--variant-steps", type=int, default=10)
+    p.add_argument("--no-configs", action="store_true",
+                   help="N=1: skip the configuration-3 and configuration-4 runs added to the line")
     p.add_argument("--accuracy-iters", type=int, default=2000,
                    help="iterations of the accuracy run of each variant (and FP32) against FP64; 0 for none")
     p.add_argument("--rate", type=float, default=6.0, help="config 5: Poisson arrival rate (requests/s)")
@@ -379,6 +383,26 @@ def storage_variants(args, stream, fp32_value, fp32_kern):
     return out
 
 
+def other_configs() -> dict:
+    """Configurations 3 and 4 in the N=1 line, so their rates are recorded with the headline:
+    configuration 3 (d3q19 porous channel 384x192x192, 5000 iterations, FP64 / FP32 / FP16-shift /
+    BF16-shift, each storage's velocity and flux error against the FP64 run) and configuration 4
+    (512 batched d2q9 cases, 2000 iterations each, FP32 and FP16-shift, the launch shape the
+    autotuner picks, 32 x 32 tiles and 64 iterations per replay, fixed here to keep the run short)."""
+    from tclb_b200 import benchmarks as BM
+
+    c3 = BM.config3()
+    c4 = BM.config4(tune=False, launch=(32, 32, 64))
+    keep = ("MLUPS", "hbm_roofline_frac", "u_rel_l2_vs_fp64", "flux_rel_err_vs_fp64")
+    out = {"config3": {"workload": c3["config"], "fp16s_speedup_vs_fp32": c3.get("fp16s_speedup_vs_fp32"),
+                       "runs": {k: {x: v[x] for x in keep if x in v} for k, v in c3["runs"].items()}},
+           "config4": {"workload": c4["config"],
+                       "runs": {k: {x: v[x] for x in ("MLUPS", "cases_per_s", "fraction_of_single",
+                                                      "single_large_case_MLUPS", "launch") if x in v}
+                                for k, v in c4["runs"].items()}}}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -478,6 +502,9 @@ def run_ours(args):
     variants = None
     if world == 1 and args.variants and args.storage == "same" and args.precision == "fp32" and args.case == "tgv":
         variants = storage_variants(args, stream, value, kern)
+    configs = None
+    if world == 1 and not args.no_configs and args.case == "tgv" and args.storage == "same":
+        configs = other_configs()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -487,6 +514,7 @@ def run_ours(args):
                 "kernel_path": "tma" if path["tma"] else ("pairs" if path["pairs"] else "one"),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": args.steps * (I + 2), "wall_s": wall, "storage_variants": variants,
+                "other_configs": configs,
                 "globals_last": dict({k: float(v) for k, v in glob.items()}, KineticEnergy=energy[0],
                                      Enstrophy=energy[1])}
         print(json.dumps(line), flush=True)

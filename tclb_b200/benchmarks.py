@@ -181,9 +181,10 @@ def aggregate_batch(reps, updates: float, seconds: float, ncases: int, single: f
             "single_large_case_MLUPS": single_mean, "fraction_of_single": mlups / (reps.world * single_mean)}
 
 
-def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True, reps=None) -> dict:
+def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True, reps=None, launch=None) -> dict:
     """With reps over N > 1 ranks (one GPU each) the cases are shared out by
-    work (replicas.partition_cases), with no exchange between the ranks."""
+    work (replicas.partition_cases), with no exchange between the ranks.
+    launch = (bx, by, K) fixes the launch shape instead of autotuning."""
     from .replicas import Replicas, partition_cases
 
     reps = reps or Replicas("gloo")
@@ -204,6 +205,8 @@ def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True,
         b.set_paths(globals_at_end=True)  # Globals of each case's last iteration only
         if tuned:
             b.set_launch(tuned["bx"], tuned["by"], tuned["K"])
+        elif launch:
+            b.set_launch(*launch)
         t_add = time.perf_counter()
         ids = [b.add_case(s) for s in specs]
         t_add = time.perf_counter() - t_add
