@@ -24,9 +24,11 @@ configuration 4 (512 batched d2q9 cases, FP32 and FP16-shift).
 Multi-GPU (torchrun, one rank per GPU): independent replicas, weak scaling, no
 data-path collective (the case does not shard across GPUs here).
 
-``--impl reference`` times the CPU restatement of the reference path (the
-oracle; TCLB itself cannot be built without R/polyAlgebra/MPI) on the host
-cores on a bounded slab of the same workload.
+``--impl reference`` times the reference's CPU path on the host cores on a
+bounded slab of the same workload, K steps: TCLB's own d3q27_cumulant node
+code (CollisionMRT compiled from its source into oracle/_ref) in a pull-stream
+loop when that library is built, else the oracle (the CPU restatement; TCLB as
+a whole cannot be built without R/polyAlgebra/MPI).
 """
 from __future__ import annotations
 
@@ -210,9 +212,56 @@ def case_lattice(args, precision=None, storage=None):
     return lat
 
 
+def ref_cpu_baseline(args, seconds, threads=None):
+    """TCLB's own d3q27_cumulant node code (CollisionMRT, models/flow/d3q27_cumulant/Dynamics.c.Rt:309-519,
+    compiled from the reference's source into oracle/_ref by oracle/make_ref.py) in a pull-stream loop over a
+    slab of the workload (256 x 256 x cpu_slab nodes, periodic, OpenMP over rows); None if that library is
+    not on this machine."""
+    try:
+        from oracle import make_ref, ref
+        if not os.path.exists(make_ref.LIB):
+            return None
+        cores = ref.threads(threads or os.cpu_count() or 1)
+    except Exception:
+        return None
+    from tclb_b200 import cases
+    from tclb_b200 import models as M
+
+    n, nz = args.n, args.cpu_slab
+    dt = np.float64 if args.precision == "fp64" else np.float32
+    m = M.get("d3q27_cumulant")
+    rho, u = cases.tgv_fields(n, u0=0.05, nz=nz, dtype=np.float64)
+    J = rho[..., None] * u
+    e = np.array(m.velocities, float)
+    w = np.array(m.weights)
+    eu = np.einsum("qd,zyxd->qzyx", e, J)
+    a = np.ascontiguousarray(w[:, None, None, None] * (rho + 3 * eu + 4.5 * eu ** 2 / rho - 1.5 * (J ** 2).sum(-1) / rho),
+                             dtype=dt)
+    b = np.empty_like(a)
+    S = {"nu": TGV_NU["d3q27_cumulant"]}
+    ref.d3q27c_iterate(a, b, S)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        ref.d3q27c_iterate(a, b, S)
+        a, b = b, a
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and done >= 2:
+            break
+    return {"value": n * n * nz * done / el / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"d3q27_cumulant TGV slab {n}x{n}x{nz}, {done} iterations in {el:.1f} s, {args.precision}: "
+                      "TCLB's CollisionMRT compiled from its source (oracle/make_ref.py) in a pull-stream loop, "
+                      "OpenMP over rows (TCLB's own build needs R+polyAlgebra, autoconf, MPI)"}
+
+
 def cpu_baseline(args, model_name, seconds, threads=None):
-    """The oracle (CPU restatement of the reference path) on a slab of the
-    workload: 256 x 256 x cpu_slab nodes, periodic, same settings."""
+    """The reference's CPU path on a slab of the workload: TCLB's own node code (oracle/_ref) for
+    d3q27_cumulant when it is built here, else the oracle (CPU restatement of the path): 256 x 256 x
+    cpu_slab nodes, periodic, same settings."""
+    if model_name == "d3q27_cumulant":
+        r = ref_cpu_baseline(args, seconds, threads)
+        if r is not None:
+            return r
     import oracle
     from tclb_b200 import cases
     from tclb_b200 import models as M
@@ -271,16 +320,13 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    import oracle
-
-    cores = oracle.set_threads(os.cpu_count() or 1)
-    # each step a bounded sample (about cpu_seconds / 4 of CPU time)
-    per = max(1.0, args.cpu_seconds / 4)
+    # K steps, each a bounded sample of the workload (at most cpu_seconds / 4, and 120 s over all steps)
+    per = max(0.5, min(args.cpu_seconds / 4, 120.0 / max(1, args.steps)))
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_baseline(args, args.model, 0.5)
     vals = []
     t_all = time.perf_counter()
-    for _ in range(args.steps if args.steps <= 5 else 5):
+    for _ in range(args.steps):
         r = cpu_baseline(args, args.model, per)
         vals.append(r["value"])
     el = time.perf_counter() - t_all
@@ -290,7 +336,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
             "impl": "reference",
             "config": workload_config(args, world),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "gpu_launches": 0}

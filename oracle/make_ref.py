@@ -433,7 +433,11 @@ def generate(ref: str) -> str:
 
 HEADER = """// Generated by oracle/make_ref.py from TCLB's model sources. Test infrastructure only; not committed.
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #define CudaDeviceFunction
 using std::sqrt;
 """
@@ -550,10 +554,58 @@ void d2q9srt(int op, int n, double* f, const double* s) {
     for (int i = 0; i < 9; i++) f[9 * k + i] = m.f[i];
   }
 }
+// One iteration of a periodic lattice of all-MRT, untyped-boundary nodes: node
+// x takes f_i from x - e_i (index i = a + 3b + 9c over digits 0, +1, -1), then
+// TCLB's CollisionMRT. The loop is this harness's; the node code is TCLB's.
+template <class R, class real>
+void d3q27c_iterate(int nx, int ny, int nz, const real* src, real* dst, const double* s) {
+  const size_t N = (size_t)nx * ny * nz;
+  static const int dg[3] = {0, 1, -1};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++) {
+      const real* row[27];  // the source row of each population (y and z wrapped once per row)
+      int ex[27];
+      for (int i = 0; i < 27; i++) {
+        const int ey = dg[(i / 3) % 3], ez = dg[i / 9];
+        const int ys = (y - ey + ny) % ny, zs = (z - ez + nz) % nz;
+        row[i] = src + (size_t)i * N + (size_t)nx * (ys + (size_t)ny * zs);
+        ex[i] = dg[i % 3];
+      }
+      for (int x = 0; x < nx; x++) {
+        R m;
+        for (int i = 0; i < 27; i++) {
+          int xs = x - ex[i];
+          xs = xs < 0 ? xs + nx : (xs >= nx ? xs - nx : xs);
+          *m.fp(i) = row[i][xs];
+        }
+        m.nu = s[0]; m.nubuffer = s[1]; m.GalileanCorrection = s[2];
+        m.ForceX = s[3]; m.ForceY = s[4]; m.ForceZ = s[5]; m.Omega = s[6];
+        m.NodeType = 0;
+        for (int g = 0; g < 6; g++) m.G[g] = 0;
+        m.CollisionMRT();
+        const size_t n = x + (size_t)nx * (y + (size_t)ny * z);
+        for (int i = 0; i < 27; i++) dst[(size_t)i * N + n] = *m.fp(i);
+      }
+    }
+}
 }  // namespace
 
 extern "C" {
-int ref_version() { return 1; }
+int ref_version() { return 2; }
+int ref_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+int ref_d3q27c_iterate(int fp64, int nx, int ny, int nz, const void* src, void* dst, const double* s) {
+  if (fp64) d3q27c_iterate<ref64::D3Q27C, double>(nx, ny, nz, (const double*)src, (double*)dst, s);
+  else d3q27c_iterate<ref32::D3Q27C, float>(nx, ny, nz, (const float*)src, (float*)dst, s);
+  return 0;
+}
 int ref_d3q27c_collide(int fp64, int n, double* f, const double* s, const int* boundary, double* glob) {
   if (fp64) d3q27c_collide<ref64::D3Q27C>(n, f, s, boundary, glob); else d3q27c_collide<ref32::D3Q27C>(n, f, s, boundary, glob);
   return 0;
@@ -586,7 +638,8 @@ def build(ref: str = DEFAULT_REF, force: bool = False, verbose: bool = False) ->
     src = generate(ref)
     with open(GEN, "w") as fh:
         fh.write(src)
-    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-Wno-narrowing", "-w", "-o", LIB, GEN]
+    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off", "-Wno-narrowing", "-w",
+           "-o", LIB, GEN]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

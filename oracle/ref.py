@@ -46,6 +46,8 @@ def lib():
         L.ref_d3q27c_rho_u.argtypes = [i, i, vp, vp, vp]
         L.ref_d3q19_boundary.argtypes = [i, i, i, vp, vp]
         L.ref_d2q9srt.argtypes = [i, i, i, vp, vp]
+        L.ref_threads.argtypes = [i]
+        L.ref_d3q27c_iterate.argtypes = [i, i, i, i, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -107,3 +109,22 @@ def d2q9srt(op: str, f, omega=1.0, velocity_x=0.0, velocity_y=0.0, density=1.0, 
     s = np.array([omega, velocity_x, velocity_y, density, grav_x, grav_y], np.float64)
     lib().ref_d2q9srt(_fp64(precision), D2Q9_OPS[op], a.shape[0], a.ctypes.data, s.ctypes.data)
     return a
+
+
+def threads(n: int = 0) -> int:
+    """Set (n > 0) and return the OpenMP threads of the lattice loop."""
+    return lib().ref_threads(int(n))
+
+
+def d3q27c_iterate(src, dst, settings: dict):
+    """One iteration of a periodic all-MRT d3q27_cumulant lattice (Q, nz, ny, nx), float64 or float32:
+    pull-stream in this harness's loop, then TCLB's CollisionMRT at every node. Writes dst."""
+    if src.dtype != dst.dtype or src.shape != dst.shape or src.shape[0] != 27 or src.dtype not in (np.float64,
+                                                                                                     np.float32):
+        raise ValueError("src and dst: (27, nz, ny, nx) arrays of one float type")
+    if not (src.flags.c_contiguous and dst.flags.c_contiguous):
+        raise ValueError("contiguous arrays needed")
+    s = np.array([float(settings.get(k, d)) for k, d in zip(D3Q27C_SETTINGS, (1 / 6, 0.01, 1.0, 0, 0, 0, 1.0))])
+    _, nz, ny, nx = src.shape
+    lib().ref_d3q27c_iterate(1 if src.dtype == np.float64 else 0, nx, ny, nz, src.ctypes.data, dst.ctypes.data,
+                             s.ctypes.data)

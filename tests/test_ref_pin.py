@@ -142,3 +142,22 @@ def test_oracle_d2q9_init_vs_golden(prec):
     f = o.densities().reshape(9, -1)
     exp = fx[f"d2q9_init_{prec}"]
     assert np.max(np.abs(f - exp[:, None])) < BARS[prec] * np.max(np.abs(exp))
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_ref_lattice_loop_matches_oracle(prec):
+    """The CPU baseline's loop (pull-stream + TCLB's CollisionMRT over a periodic lattice) is one
+    iteration of the oracle lattice on an all-MRT flag field."""
+    n = 12
+    dt = np.float64 if prec == "fp64" else np.float32
+    a = np.ascontiguousarray(G.near_equilibrium("d3q27_cumulant", (n, n, n), 3, 0.05).astype(dt))
+    b = np.empty_like(a)
+    ref.d3q27c_iterate(a, b, G.D3Q27C_SET)
+    o = oracle.OracleLattice("d3q27_cumulant", n, n, n, precision=prec)
+    o.set_flags(np.full((n, n, n), M.get("d3q27_cumulant").flag("MRT"), np.uint16))
+    for k, v in G.D3Q27C_SET.items():
+        o.set_setting(k, v)
+    o.set_densities(a.astype(np.float64))
+    o.iterate(1)
+    assert G.rel_l2(b, o.densities()) < BARS[prec]
