@@ -194,8 +194,9 @@ int tclb_sync(tclb_h h);
 #define TCLB_LAUNCH_PAIRS 2
 #define TCLB_LAUNCH_TMA 4
 /* With TCLB_LAUNCH_TMA: stage tiles wherever the tile-staged kernel applies,
-   also for d3q19 rows wider than 256, which otherwise take the register pair
-   kernel (measured faster there). */
+   also where d3q19 otherwise takes the register pair kernel (nx % 64 == 0 and
+   rows wider than 256, tiles of fewer than 448 nodes, or fewer than four tiles
+   per resident block: measured faster there). */
 #define TCLB_LAUNCH_TMA_ALWAYS 8
 int tclb_set_launch(tclb_h h, int bx, int by, int flags);
 /* The launch shape and the paths plain iterations take on this lattice: the
@@ -251,6 +252,15 @@ size_t tclb_batch_case_bytes(int model, int precision, int storage, int nx, int 
    budget_bytes and at most max_cases are resident. */
 int tclb_batch_create(tclb_batch_h* out, int model, int precision, int storage, size_t budget_bytes, int max_cases);
 int tclb_batch_destroy(tclb_batch_h b);
+/* Grow the batch's device memory pool to hold at least `bytes` (at most the
+   budget) for the cases it will admit: blocks of up to 2 GiB are allocated
+   and freed back to the pool, which keeps freed memory. Admissions that fit
+   the reserve then take memory from the pool without mapping new device
+   memory, which otherwise costs milliseconds per case, and at times hundreds
+   of milliseconds, while other work runs. Returns after the pool has grown;
+   TCLB_ERR_MEMORY if the device cannot provide it (the pool keeps what it
+   got). The reserve does not count against the budget. No TCLB counterpart. */
+int tclb_batch_reserve(tclb_batch_h b, size_t bytes);
 
 /* Admit a case: node types (x fastest), the full Settings vector (derived
    chains already applied), `zone_rows` rows of ZoneSettings (zone 0..), and

@@ -34,6 +34,7 @@ def _lib():
         L.tclb_batch_case_bytes.restype = sz
         L.tclb_batch_create.argtypes = [ctypes.POINTER(h), i, i, i, sz, i]
         L.tclb_batch_destroy.argtypes = [h]
+        L.tclb_batch_reserve.argtypes = [h, sz]
         L.tclb_batch_add_case.argtypes = [h, i, i, i, ctypes.POINTER(ctypes.c_uint16), dp, dp, i, i, ip]
         L.tclb_batch_remove_case.argtypes = [h, i]
         L.tclb_batch_set_launch.argtypes = [h, i, i, i, i]
@@ -109,6 +110,14 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+    def reserve(self, nbytes: int):
+        """Grow the device memory pool to hold nbytes for future cases (at most the budget), so that
+        admissions within it do not map new device memory (tclb_batch_reserve)."""
+        rc = self.lib.tclb_batch_reserve(self._h, int(nbytes))
+        if rc == -3:
+            raise AdmissionRefused(self.lib.tclb_batch_last_error().decode())
+        _check(rc)
 
     # -- cases -----------------------------------------------------------------
     def settings_vector(self, settings: Dict[str, float]) -> np.ndarray:

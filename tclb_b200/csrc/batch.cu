@@ -76,6 +76,9 @@ struct BatchImpl {
   const void* (*tile_kernel)(int which);  // 0 one-tile plain, 1 one-tile Globals, 2 pair
   int pair_threads;                        // block-size limit of the pair kernel; 0: no pair kernel
   bool group_staging;                      // staged cases must share their settings (packed collision)
+  // smallest staged tile (nodes) of a case; cases with smaller tiles take the
+  // register kernels (0: any tile)
+  int min_staged_nodes;
   size_t real_size;
   int Q, NG, NSET, NZS, zone_shift;
 };
@@ -184,6 +187,11 @@ struct BL {
     k_quantity<M, R, St><<<grd, dim3(32, 4), 0, s>>>(a, q, vec, 0, 0, 0, C.nx, C.ny, C.nz, (R)scale,
                                                       static_cast<R*>(out));
   }
+  // d3q19's register pair kernel (identity-rate lanes) measured faster than
+  // staged tiles that leave more than an eighth of the consumer threads idle
+  // (B200, porous boxes in batches: edge 160, 320-node tiles: 43.4k against
+  // 38.9k MLUPS; edge 192, 384-node tiles: 49.7k against 42.0k)
+  static constexpr int min_staged_nodes() { return M::identity_lanes ? 448 : 0; }
   static const BatchImpl* get() {
     static const BatchImpl impl = {iterate,
                                    tma_grid,
@@ -195,6 +203,7 @@ struct BL {
                                    tile_kernel,
                                    pairs ? M::PAIR_THREADS : 0,
                                    M::has_bulk,
+                                   min_staged_nodes(),
                                    sizeof(R),
                                    M::Q,
                                    M::NG,
@@ -235,6 +244,14 @@ struct CaseLayout {
   size_t stride, buf, flags, zone, glob, maps, total;
 };
 
+// Rows per staged tile of a case (tma_rows_for), or 0 where the case takes
+// the register kernels: its rows do not fit a box, or its tiles are smaller
+// than the model's min_staged_nodes.
+int staged_rows(const BatchImpl* I, size_t elem, int nx, int ny) {
+  const int R = tma_rows_for(elem, nx, ny);
+  return R * nx >= I->min_staged_nodes ? R : 0;
+}
+
 // One allocation per case: two snapshots, node types, zone table, Globals,
 // and for a case the tile-staged kernel can take, its tensor maps.
 CaseLayout case_layout(const BatchImpl* I, size_t elem, int nx, int ny, int nz) {
@@ -245,7 +262,7 @@ CaseLayout case_layout(const BatchImpl* I, size_t elem, int nx, int ny, int nz) 
   L.flags = align_up(N * sizeof(flag_t), 256);
   L.zone = align_up((size_t)(1 << (16 - I->zone_shift)) * I->NZS * I->real_size, 256);
   L.glob = align_up(I->NG * sizeof(double), 256);
-  L.maps = tma_rows_for(elem, nx, ny) ? align_up(sizeof(BatchTmaMaps), 256) : 0;
+  L.maps = staged_rows(I, elem, nx, ny) ? align_up(sizeof(BatchTmaMaps), 256) : 0;
   L.total = 2 * L.buf + L.flags + L.zone + L.glob + L.maps;
   return L;
 }
@@ -561,7 +578,7 @@ int fill_case(tclb_batch* B, int slot, char* p, const CaseLayout& L, const Model
   C.glob_end = (B->paths & TCLB_BATCH_GLOBALS_AT_END) ? 1 : 0;
   BatchTmaMaps maps;  // host copy of the tensor maps, uploaded below
   if (L.maps) {
-    const int R = tma_rows_for(B->elem, nx, ny);
+    const int R = staged_rows(B->I, B->elem, nx, ny);
     bool ok = true;
     for (int b = 0; b < 2 && ok; b++)
       ok = encode_tile_maps(C.buf[b], C.flags, nx, ny, nz, B->I->Q, L.stride, R, &maps.rows[b], &maps.row1[b],
@@ -714,6 +731,27 @@ int tclb_batch_add_case(tclb_batch_h B, int nx, int ny, int nz, const uint16_t* 
   B->h_status[slot] = make_int2(0, niter);
   B->tiles_dirty = true;
   *case_id = slot;
+  return TCLB_OK;
+}
+
+int tclb_batch_reserve(tclb_batch_h B, size_t bytes) {
+  CHECK_B(B);
+  if (bytes > B->budget) return bfail(TCLB_ERR_ARG, "reserve: more than the batch's budget");
+  constexpr size_t BLOCK = (size_t)1 << 31;
+  std::vector<void*> blocks;
+  cudaError_t e = cudaSuccess;
+  for (size_t done = 0; done < bytes && e == cudaSuccess; done += BLOCK) {
+    void* p = nullptr;
+    e = cudaMallocFromPoolAsync(&p, std::min(BLOCK, bytes - done), B->pool, B->stream);
+    if (e == cudaSuccess) blocks.push_back(p);
+  }
+  for (void* p : blocks) cudaFreeAsync(p, B->stream);  // back to the pool, which keeps them
+  const cudaError_t s = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return bfail(TCLB_ERR_MEMORY, std::string("reserve: ") + cudaGetErrorString(e));
+  }
+  BCK(s);
   return TCLB_OK;
 }
 

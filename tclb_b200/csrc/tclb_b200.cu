@@ -161,8 +161,9 @@ struct tclb_lattice {
   // 16-bit storage: tile-staged TMA kernel (tma_rows rows per tile; tma[b]
   // describes snapshot b as the source), and its error word in the pool
   int use_tma = 1, tma_ok = 0, tma_rows = 0, tma_grid = 0;
-  // rows wider than 256 of a model whose register pair kernel measured faster
-  // there (d3q19): plain iterations take that kernel unless tma_always
+  // shapes where a model's register pair kernel measured faster (d3q19: rows
+  // wider than 256, under-filled or too few tiles): plain iterations take
+  // that kernel unless tma_always
   int tma_pref_pairs = 0, tma_always = 0;
   TmaMaps tma[2];
   int* err_dev = nullptr;
@@ -267,10 +268,6 @@ struct Launch {
     using T = typename St::T;
     if constexpr (sizeof(T) == 2) {
       if (!L->tma_ok) return;
-      // d3q19 with one-row tiles (nx > 256): six consumer warps per block, and the
-      // register pair kernel with identity-rate lanes measured faster (porous
-      // 384x192x192: 57.7k against 51.3k MLUPS); narrower rows stay staged
-      if constexpr (M::identity_lanes) L->tma_pref_pairs = tma_wide(L->nx) && L->nx % 64 == 0;
       const int rows = L->tma_rows, threads = tma_threads(rows, L->nx);
       const size_t smem = tma_smem_bytes<M>();
       int per_sm = 0, sms = 0;
@@ -287,7 +284,17 @@ struct Launch {
         L->tma_ok = 0;
         return;
       }
-      L->tma_grid = std::min(L->nz * (L->ny / rows), per_sm * sms);
+      const int tiles = L->nz * (L->ny / rows);
+      L->tma_grid = std::min(tiles, per_sm * sms);
+      // d3q19 (register pair kernel with identity-rate lanes) takes that kernel
+      // where nx % 64 == 0 and the staged tiles would be under-filled or too
+      // few, as measured on B200 (porous boxes, FP16-shift): rows wider than
+      // 256 (one-row tiles, six consumer warps per block; 384x192x192: 57.7k
+      // against 51.6k MLUPS), tiles of fewer than 448 nodes (192^3: 56.4k
+      // against 50.2k), fewer than four tiles per resident block (64^3: 45.8k
+      // against 27.8k)
+      if constexpr (M::identity_lanes)
+        L->tma_pref_pairs = L->nx % 64 == 0 && (tma_wide(L->nx) || rows * L->nx < 448 || tiles < 4 * per_sm * sms);
     }
   }
   static void init(tclb_lattice* L, cudaStream_t s) {

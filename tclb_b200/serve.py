@@ -119,7 +119,13 @@ class Admission:
 class Server:
     def __init__(self, models=("d2q9", "d3q19"), precision="fp32", storage="same", budget_bytes: int = 150 << 30,
                  launch: Optional[Dict[str, Tuple[int, int, int]]] = None, max_cases: int = 4096,
-                 high_priority: Tuple[str, ...] = ("d2q9",), max_bypass_s: float = 5.0):
+                 high_priority: Tuple[str, ...] = ("d2q9",), max_bypass_s: float = 5.0,
+                 reserve: Optional[Dict[str, int]] = None):
+        """reserve: device bytes to set aside per model at start-up (Batch.reserve), so that the
+        first admissions take memory from the pools like those of a server that has been running;
+        the sum must stay within the budget."""
+        if reserve and sum(reserve.values()) > budget_bytes:
+            raise ValueError("reserve exceeds the budget")
         self.precision, self.storage = precision, storage
         self.budget = int(budget_bytes)
         self.batches: Dict[str, Batch] = {}
@@ -131,6 +137,8 @@ class Server:
                 b.set_launch(*launch[m])
             if m in high_priority:  # small cases: their blocks go first
                 b.set_priority(True)
+            if reserve and reserve.get(m):
+                b.reserve(reserve[m])
             self.batches[m] = b
         self.adm = Admission(self.budget, self.footprint, models, max_bypass_s)
         self.pending: Dict[str, List[Request]] = {m: [] for m in models}  # admitted, joining at the next boundary

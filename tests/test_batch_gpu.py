@@ -275,7 +275,8 @@ TMA_SHAPES = {
 @pytest.mark.parametrize("storage", ["fp16s", "bf16"])
 def test_batch_tile_staged_matches_pairs_bit_for_bit(model, storage):
     """Cases whose rows fit the tile-staged kernel (nx a multiple of 32 up to
-    512: here 64, 96, 128, 192, 256) take the tile-staged batch kernel, a case
+    512: here 64, 96, 128, 192, 256; for d3q19 only those whose tiles hold at
+    least 448 nodes) take the tile-staged batch kernel, a case
     with other settings the pair kernel, in one batch; every field and Globals
     vector must equal that of the same batch with staging off (the same pair
     update on the same values; nx = 96 runs its last tile of each row
@@ -374,3 +375,25 @@ def test_staging_needs_enough_tiles():
         b.close()
         return r
     assert not uses_tma(64) and uses_tma(128)
+
+
+def test_reserve_grows_the_pool_and_changes_nothing_else():
+    """tclb_batch_reserve: more than the budget is refused; a reserve within it
+    leaves admission (budget accounting) and results unchanged."""
+    from tclb_b200.lattice import TCLBError
+
+    spec = CaseSpec(cases.porous_channel_d3q19(128, 64, 32, p=0.08, band=2, seed=9), {"nu": 0.02, "ForceX": 1e-5}, {}, 12)
+    out = []
+    for reserve in (0, 256 << 20):
+        b = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=512 << 20)
+        with pytest.raises(TCLBError):
+            b.reserve(1 << 30)
+        if reserve:
+            b.reserve(reserve)
+        assert b.info()["used_bytes"] == 0
+        c = b.add_case(spec)
+        assert b.info()["used_bytes"] == case_bytes("d3q19", 128, 64, 32, "fp32", "fp16s")
+        b.run_to_completion()
+        out.append(b.quantity(c, "U"))
+        b.close()
+    assert np.array_equal(out[0], out[1])
