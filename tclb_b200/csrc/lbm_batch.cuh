@@ -351,8 +351,12 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
   unsigned phase = 0;
   int nx = 0, ny = 0, r = 0, x = 0, xm = 0, xp2 = 0;
   bool run = false, act = false;
+  // each tile's descriptor is loaded one tile ahead, so its latency overlaps
+  // the previous tile's update instead of stalling the warp at every tile
+  BatchTmaTile next = (int)blockIdx.x < ntiles ? tiles[blockIdx.x] : BatchTmaTile{0, 0, 0};
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const BatchTmaTile tile = tiles[t];
+    const BatchTmaTile tile = next;
+    if (t + (int)gridDim.x < ntiles) next = tiles[t + gridDim.x];
     if (tile.slot != slot) {  // the same for every consumer warp
       slot = tile.slot;
       const BatchCase& C = cases[slot];
