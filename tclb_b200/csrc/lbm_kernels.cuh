@@ -112,16 +112,13 @@ __device__ __forceinline__ void add_glob(R* g, int i, R x, const R* zs) {
 struct D2Q9 {
   static constexpr int Q = 9, DIM = 2, NSET = d2q9::NSET, NZS = d2q9::NZS, NG = d2q9::NG, NSUM = d2q9::NSUM,
                        ZONE_SHIFT = d2q9::ZONE_SHIFT;
-  static constexpr bool has_bulk = false;  // no packed two-node collision
+  // staged batch cases keep their own settings (no shared settings group):
+  // the cases of a batch differ in viscosity
+  static constexpr bool has_bulk = false;
+  static constexpr bool packed = true;  // one packed FP32x2 collision for a node pair
   static constexpr bool identity_lanes = false;
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 4;  // <= 64 registers
   static constexpr int BATCH_MIN_BLOCKS = 6;  // one-tile batch kernel: <= 40 registers
-  __device__ __forceinline__ static bool collides(flag_t) { return false; }
-  __device__ __forceinline__ static bool has_boundary(flag_t) { return false; }
-  template <class R, class AR>
-  __device__ __forceinline__ static void pre_collision(R (&)[Q], flag_t, const AR&) {}
-  template <bool DEV, class AR>
-  __device__ __forceinline__ static void collide_pair(F2 (&)[Q], flag_t, flag_t, const AR&) {}
   template <class R>
   __host__ __device__ static void derived(const R*, R* k) { k[0] = k[1] = k[2] = k[3] = R(0); }
   __host__ __device__ static constexpr int ex(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0); }
@@ -232,9 +229,15 @@ struct D2Q9 {
 
   template <class R, bool G>
   __device__ __forceinline__ static void run(R (&f)[Q], flag_t fl, const Args<R, NSET>& a, R* g) {
-    const R* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
+    boundaries(f, fl, a);
+    if (fl & d2q9::MRT) mrt<R, G>(f, fl, a, g, a.zone + (fl >> ZONE_SHIFT) * NZS);
+  }
+
+  template <class R, class AR>
+  __device__ __forceinline__ static void boundaries(R (&f)[Q], flag_t fl, const AR& a) {
     const unsigned b = fl & d2q9::BOUNDARY;
     if (b) {
+      const auto* zs = a.zone + (fl >> ZONE_SHIFT) * NZS;
       const R vx = zs[d2q9::Z_VelocityX], vy = zs[d2q9::Z_VelocityY], rho0 = zs[d2q9::Z_Pressure] * R(3) + R(1);
       switch (b) {  // d2q9/Dynamics.c.Rt:108-138
         case d2q9::Solid:
@@ -250,8 +253,53 @@ struct D2Q9 {
         default: break;
       }
     }
-    if (fl & d2q9::MRT) mrt<R, G>(f, fl, a, g, zs);
   }
+
+  // Two nodes with one packed collision (plain iterations): boundaries per
+  // node, then the MRT update of mrt() on both lanes; a lane whose node does
+  // not collide keeps its values (pair_update_store parks them). With DEV the
+  // values are deviations g = f - w: the weights' MRT moments are all zero
+  // but the density (1), so the moments of g are those of f with rho - 1,
+  // which enters the linear terms (from_moments is linear, its rho part
+  // weighted by w), while the quadratic equilibrium terms and the force use
+  // the true density.
+  __device__ __forceinline__ static bool collides(flag_t fl) { return (fl & d2q9::MRT) != 0; }
+  __device__ __forceinline__ static bool has_boundary(flag_t fl) { return (fl & d2q9::BOUNDARY) != 0; }
+  template <class R, class AR>
+  __device__ __forceinline__ static void pre_collision(R (&f)[Q], flag_t fl, const AR& a) {
+    boundaries(f, fl, a);
+  }
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair(F2 (&f)[Q], flag_t, flag_t, const AR& a) {
+    const F2 d = f[5] + f[6] + f[7] + f[8];
+    const F2 rho = f[0] + f[1] + f[2] + f[3] + f[4] + d;  // rho - 1 with DEV
+    F2 jx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    F2 jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    F2 m3 = -f[0] + F2(2.0f) * (f[1] + f[3]) - f[2] - f[4] + F2(2.0f) * d;
+    F2 m4 = -f[0] - f[1] - f[3] + F2(2.0f) * (f[2] + f[4]) + F2(2.0f) * d;
+    F2 m5 = F2(3.0f) * (f[5] - f[6] + f[7] - f[8]);
+    F2 m6 = f[4] - f[2] + F2(2.0f) * (f[5] + f[6] - f[7] - f[8]);
+    F2 m7 = f[3] - f[1] + F2(2.0f) * (f[5] - f[6] - f[7] + f[8]);
+    F2 m8 = f[0] - F2(2.0f) * (f[1] + f[2] + f[3] + f[4]) + F2(4.0f) * d;
+    const F2 rho_t = DEV ? rho + F2(1.0f) : rho;  // true density
+    const F2 irho = recip(rho_t);
+    const F2 S2((float)a.s[d2q9::S_S2]), S3((float)a.s[d2q9::S_S3]), S4((float)a.s[d2q9::S_S4]);
+    const F2 gx((float)a.s[d2q9::S_GravitationX]), gy((float)a.s[d2q9::S_GravitationY]);
+    m3 = S2 * (m3 - F2(3.0f) * jx * jx * irho);
+    m4 = S2 * (m4 - F2(3.0f) * jy * jy * irho);
+    m5 = S2 * (m5 - F2(3.0f) * jx * jy * irho);
+    m6 = S3 * m6;
+    m7 = S3 * m7;
+    m8 = S4 * m8;
+    jx = jx + gx * rho_t;
+    jy = jy + gy * rho_t;
+    m3 += F2(3.0f) * jx * jx * irho;
+    m4 += F2(3.0f) * jy * jy * irho;
+    m5 += F2(3.0f) * jx * jy * irho;
+    from_moments(f, rho, jx, jy, m3, m4, m5, m6, m7, m8);
+  }
+  template <bool DEV, class AR>
+  __device__ __forceinline__ static void collide_pair_lanes(F2 (&)[Q], bool, bool, const AR&) {}
 
   // SetEquilibrum (:73-89): f = Req(rho, J) in the MRT basis, mapped back
   template <class R>
@@ -292,6 +340,7 @@ struct D3Q19 {
   static constexpr int Q = 19, DIM = 3, NSET = d3q19::NSET, NZS = d3q19::NZS, NG = d3q19::NG, NSUM = d3q19::NSUM,
                        ZONE_SHIFT = d3q19::ZONE_SHIFT;
   static constexpr bool has_bulk = true;
+  static constexpr bool packed = true;
   // two-node kernel: 256 threads, <= 80 registers (3 blocks per SM), no spills
   static constexpr int PAIR_THREADS = 256, PAIR_MIN_BLOCKS = 3;
   static constexpr int BATCH_MIN_BLOCKS = 5;  // one-tile batch kernel: <= 48 registers
@@ -632,6 +681,7 @@ struct D3Q27C {
   static constexpr int Q = 27, DIM = 3, NSET = d3q27c::NSET, NZS = d3q27c::NZS, NG = d3q27c::NG,
                        NSUM = d3q27c::NSUM, ZONE_SHIFT = d3q27c::ZONE_SHIFT;
   static constexpr bool has_bulk = true;
+  static constexpr bool packed = true;
   // two-node kernel: 128 threads, <= 96 registers (5 blocks per SM), no spills
   static constexpr int PAIR_THREADS = 128, PAIR_MIN_BLOCKS = 5;
   static constexpr int BATCH_MIN_BLOCKS = 4;  // one-tile batch kernel: <= 64 registers
@@ -1088,7 +1138,7 @@ template <class M, class R, class St, class A, class AR, bool LANES = false>
 __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb, const AR& a, const A& P,
                                                   unsigned node) {
   using P16 = Pack16<St>;
-  if constexpr (M::has_bulk && sizeof(R) == 4) {
+  if constexpr (M::packed && sizeof(R) == 4) {
     // Values stay packed (node x, node x+1). A node with a boundary type has
     // its lane taken out, updated by the scalar boundary code and put back;
     // then one packed FP32x2 collision serves both nodes, so bulk and
