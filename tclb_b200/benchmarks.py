@@ -184,7 +184,8 @@ def aggregate_batch(reps, updates: float, seconds: float, ncases: int, single: f
 def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True, reps=None, launch=None) -> dict:
     """With reps over N > 1 ranks (one GPU each) the cases are shared out by
     work (replicas.partition_cases), with no exchange between the ranks.
-    launch = (bx, by, K) fixes the launch shape instead of autotuning."""
+    launch = (bx, by, K), or a dict of them by storage, fixes the launch shape
+    instead of autotuning."""
     from .replicas import Replicas, partition_cases
 
     reps = reps or Replicas("gloo")
@@ -203,10 +204,11 @@ def config4(n_cases=512, iterations=2000, storages=("same", "fp16s"), tune=True,
             tuned = autotune("d2q9", sample, precision="fp32", storage=st, trial_iters=64, globals_at_end=True)
         b = Batch("d2q9", "fp32", storage=st, budget_bytes=100 << 30, max_cases=max(1, len(specs)))
         b.set_paths(globals_at_end=True)  # Globals of each case's last iteration only
+        fixed = launch.get(st) if isinstance(launch, dict) else launch
         if tuned:
             b.set_launch(tuned["bx"], tuned["by"], tuned["K"])
-        elif launch:
-            b.set_launch(*launch)
+        elif fixed:
+            b.set_launch(*fixed)
         t_add = time.perf_counter()
         ids = [b.add_case(s) for s in specs]
         t_add = time.perf_counter() - t_add
