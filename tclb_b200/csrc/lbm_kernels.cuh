@@ -1272,8 +1272,19 @@ __global__ void __launch_bounds__(M::PAIR_THREADS, M::PAIR_MIN_BLOCKS)
   if (y < a.ny) node_update_pair<M, R, St, PlaneAddr<typename St::T, M::Q>>(a, P, x, y, z, lane);  // y is uniform per warp
 }
 
+// Launched with programmatic stream serialization (launch_pdl), the next
+// iteration's grid is scheduled while this one drains: griddepcontrol.wait
+// returns once the previous grid has completed and its writes are visible,
+// and launch_dependents lets the next grid start launching at once. Both are
+// no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait_and_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <class M, class R, class St, bool G, class A>
 __global__ void __launch_bounds__(256) k_iterate(const Args<R, M::NSET> a, const A P) {
+  pdl_wait_and_release();
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;

@@ -16,6 +16,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <utility>
 
 #include "../../include/tclb_b200.h"
 #include "lbm_tma.cuh"
@@ -210,6 +211,24 @@ inline bool tma_path(const tclb_lattice* L) {
          (L->tma_always || !L->tma_pref_pairs || !(L->use_pairs && L->nx % 64 == 0));
 }
 
+// A kernel launch on stream s whose grid may be scheduled while the previous
+// kernel on the stream drains (the kernel itself waits for it with
+// griddepcontrol.wait); captured into CUDA graphs as a programmatic edge.
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 inline dim3 grid_of(const tclb_lattice* L) {
   return dim3((L->nx + L->bx - 1) / L->bx, (L->ny + L->by - 1) / L->by, L->nz);
 }
@@ -254,12 +273,12 @@ struct Launch {
         k_iterate_pair<M, R, St><<<grd, blk, 0, s>>>(a, P);
         return;
       }
-      if (glob) k_iterate<M, R, St, true><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
-      else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
+      if (glob) launch_pdl(k_iterate<M, R, St, true, PlaneAddr<T, M::Q>>, grid_of(L), dim3(L->bx, L->by), s, a, P);
+      else launch_pdl(k_iterate<M, R, St, false, PlaneAddr<T, M::Q>>, grid_of(L), dim3(L->bx, L->by), s, a, P);
     } else {
       const StrideAddr<T> P{static_cast<const T*>(src), static_cast<T*>(dst), L->stride};
-      if (glob) k_iterate<M, R, St, true><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
-      else k_iterate<M, R, St, false><<<grid_of(L), dim3(L->bx, L->by), 0, s>>>(a, P);
+      if (glob) launch_pdl(k_iterate<M, R, St, true, StrideAddr<T>>, grid_of(L), dim3(L->bx, L->by), s, a, P);
+      else launch_pdl(k_iterate<M, R, St, false, StrideAddr<T>>, grid_of(L), dim3(L->bx, L->by), s, a, P);
     }
   }
   // Once at creation: the dynamic shared-memory limit and persistent grid of the
