@@ -404,3 +404,19 @@ def test_reserve_grows_the_pool_and_changes_nothing_else():
         out.append(b.quantity(c, "U"))
         b.close()
     assert np.array_equal(out[0], out[1])
+
+
+def test_d3q19_cases_with_underfilled_tiles_take_the_pair_kernel():
+    """In a batch, a d3q19 case whose staged tiles would hold fewer than 448 nodes
+    (edge 192: 2 rows of 192) takes the register pair kernel; a 256-edge case is
+    staged. Both give the single-lattice result."""
+    def uses(n):
+        b = Batch("d3q19", "fp32", storage="fp16s", budget_bytes=8 << 30)
+        b.set_paths(adaptive=False)
+        b.set_launch(64, 64, 4)
+        b.add_case(CaseSpec(cases.porous_channel_d3q19(n, n, 16, p=0.05, band=2, seed=3), {"nu": 0.02}, {}, 4))
+        r = (b.uses_tma(), b.uses_pairs())
+        b.close()
+        return r
+    assert uses(192) == (False, True)
+    assert uses(256)[0]

@@ -117,3 +117,27 @@ def test_tile_staged_long_run_stays_identical():
     _, (raw_tma, _, _) = run(model, shape, storage, fl, f0, tma=True, pairs=True, niter=130)
     _, (raw_pair, _, _) = run(model, shape, storage, fl, f0, tma=False, pairs=True, niter=130)
     assert raw_tma.tobytes() == raw_pair.tobytes()
+
+
+def test_d3q19_path_choice():
+    """d3q19 16-bit lattices with nx % 64 == 0 take the register pair kernel where
+    whole-row tiles would be under-filled (fewer than 448 nodes), too few (fewer
+    than four per resident block) or one row wider than 256; full tiles stay
+    staged. TCLB_LAUNCH_TMA_ALWAYS stages them anyway."""
+    def path(nx, ny, nz, always=False):
+        g = Lattice("d3q19", nx, ny, nz, precision="fp32", storage="fp16s")
+        if always:
+            g.set_launch(128, 2, use_tma=True, tma_always=True)
+        p = g.launch_path()
+        g.close()
+        return "tma" if p["tma"] else ("pairs" if p["pairs"] else "one")
+
+    assert path(256, 256, 64) == "tma"      # 2-row tiles of 512 nodes, many of them
+    assert path(192, 192, 64) == "pairs"    # 2-row tiles of 384 nodes
+    assert path(384, 64, 64) == "pairs"     # one row wider than 256
+    assert path(64, 64, 64) == "pairs"      # 512 tiles: fewer than four per resident block
+    assert path(192, 192, 64, always=True) == "tma"
+    assert path(160, 160, 32) == "tma"      # nx % 64 != 0: no pair kernel, staged
+    g = Lattice("d3q27_cumulant", 192, 192, 16, precision="fp32", storage="fp16s")
+    assert g.launch_path()["tma"]            # the rule is d3q19's
+    g.close()
