@@ -4,8 +4,8 @@ The oracle can round every stored population through a storage format
 (OracleLattice.set_storage: decode(encode(f - w_i)) + w_i, the collision in
 FP64). With it the error of a format against the plain FP64 run can be
 measured on the CPU and compared across formats that differ in one respect.
-These tests pin the findings that DESIGN.md's accuracy section rests on, on a
-small Taylor-Green vortex (d3q27_cumulant, 20^3, u0 = 0.05, nu = 1e-3, 400
+These tests pin the findings on the accuracy of 16-bit storage, on a small
+Taylor-Green vortex (d3q27_cumulant, 20^3, u0 = 0.05, nu = 1e-3, 400
 iterations):
 
 * FP16-shift storage errs as IEEE half's spacing predicts: rounding the same
