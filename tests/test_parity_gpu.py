@@ -327,3 +327,39 @@ def test_two_nodes_per_thread_path(model, storage):
     assert rel_l2(outs[1][0], outs[0][0]) < 1e-3
     e_single, e_pair = rel_l2(outs[0][0], ref), rel_l2(outs[1][0], ref)
     assert e_pair < 1.5 * e_single + 1e-6, (e_single, e_pair)
+
+
+DEGENERATE = {2: [(1, 1, 1), (1, 1, 5), (1, 3, 1), (1, 7, 33)],
+              3: [(1, 1, 1), (1, 1, 7), (3, 1, 5), (1, 4, 1), (2, 2, 33), (5, 3, 1)]}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16s"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_degenerate_shapes(model, precision):
+    """Lattices of one node, and with one or two nodes along an axis (the periodic
+    pull then reads the node itself or its one neighbour from both sides), and a
+    width that is not a multiple of 32: every boundary type on random nodes, four
+    iterations, Globals on the last, against the oracle. 16-bit storage against the
+    FP64 oracle within the storage bar."""
+    m = M.get(model)
+    for k, shape in enumerate(DEGENERATE[m.dim]):
+        fl = random_flags(model, shape, BOUNDARY_TYPES[model], zones=3, seed=40 + k, p_type=0.3,
+                          extra_groups=EXTRA_GROUPS[model])
+        f0 = perturbed_equilibrium(model, shape, seed=50 + k)
+        nz, ny, nx = shape
+        prec = "fp32" if precision == "fp16s" else precision
+        g = Lattice(model, nx, ny, nz, precision=prec, storage="fp16s" if precision == "fp16s" else "same")
+        o = oracle.OracleLattice(model, nx, ny, nz, precision="fp64" if precision != "fp32" else "fp32")
+        for lat in (g, o):
+            lat.set_flags(fl)
+            apply_params(lat, PARAMS[model])
+            lat.set_densities(f0)
+        run_both(g, o, 4, M.ITER_NORM | M.ITER_LASTGLOB)
+        f_g, f_o = g.densities(), o.densities()
+        assert np.isfinite(f_g).all(), shape
+        bar = {"fp64": TOL_F["fp64"], "fp32": TOL_F["fp32"], "fp16s": 2e-3}[precision]
+        assert rel_l2(f_g, f_o) < bar, (shape, rel_l2(f_g, f_o))
+        if precision != "fp16s":
+            ge, gg, og = compare_globals(g, o, precision)
+            assert ge < TOL_G[precision], (shape, gg, og)
+        g.close()
