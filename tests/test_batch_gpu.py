@@ -420,3 +420,29 @@ def test_d3q19_cases_with_underfilled_tiles_take_the_pair_kernel():
         return r
     assert uses(192) == (False, True)
     assert uses(256)[0]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("model", ["d2q9", "d3q19", "d3q27_cumulant"])
+def test_degenerate_cases_in_a_batch(model, precision):
+    """Cases of one node, with axes of one or two nodes, and widths that are not a
+    multiple of 32, batched together with a regular case: each case's velocity and
+    Globals equal its single-lattice run."""
+    m = M.get(model)
+    shapes = [(1, 1, 1), (1, 1, 5), (1, 3, 1), (1, 7, 33), (1, 16, 64)] if m.dim == 2 else \
+        [(1, 1, 1), (1, 1, 7), (3, 1, 5), (1, 4, 1), (2, 2, 33), (4, 8, 32)]
+    specs = [_random_case(model, sh, seed=80 + i, niter=7) for i, sh in enumerate(shapes)]
+    b = Batch(model, precision, budget_bytes=1 << 30)
+    b.set_launch(32, 4, 3)
+    ids = [b.add_case(s) for s in specs]
+    b.run_to_completion()
+    for cid, s in zip(ids, specs):
+        u_s, g_s = run_single(model, s, precision)
+        u_b, g_b = b.quantity(cid, "U"), b.globals(cid)
+        assert np.isfinite(u_b).all()
+        if np.abs(u_s).max() > 0:
+            assert rel_l2(u_b, u_s) <= TOL_U[precision], (s.shape, rel_l2(u_b, u_s))
+        else:
+            assert np.abs(u_b).max() <= 1e-12, s.shape
+        assert np.allclose(g_b, g_s, rtol=1e-9 if precision == "fp64" else 1e-4, atol=1e-12), (s.shape, g_b, g_s)
+    b.close()
