@@ -1260,6 +1260,21 @@ __device__ __forceinline__ void node_update_pair(const Args<R, M::NSET>& a, cons
   if (!PARTIAL || store) pair_update_store<M, R, St, A, Args<R, M::NSET>, true>(v, fla, flb, a, P, node);
 }
 
+// Node pairs (2p, 2p+1) of the flat node index, p < npairs, of which exactly
+// one node collides (a pair of one row when nx is even); the count is added
+// to *count.
+template <class M>
+__global__ void k_count_mixed_pairs(const flag_t* __restrict__ flags, unsigned npairs, unsigned* count) {
+  unsigned c = 0;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+    const unsigned w = __ldg(reinterpret_cast<const unsigned*>(flags) + p);
+    c += M::collides((flag_t)(w & 0xffffu)) != M::collides((flag_t)(w >> 16)) ? 1u : 0u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 // Block (32, M::PAIR_THREADS / 32): each warp covers 64 consecutive x of one
 // row. Plain iterations only (Globals iterations use k_iterate).
 template <class M, class R, class St>

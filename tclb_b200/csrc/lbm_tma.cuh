@@ -284,7 +284,7 @@ constexpr int TMA_THREADS = (TMA_CONSUMERS + 1) * 32;
 // the waits keep the compile-time bound.
 // PARTIAL: the tile's pairs do not fill whole warps (R * nx / 2 not a
 // multiple of 32), so consumer threads check that they hold a pair.
-template <class M, class R, class St, bool FAULT = false, bool PARTIAL = false>
+template <class M, class R, class St, bool FAULT = false, bool PARTIAL = false, bool LANES = false>
 __global__ void __launch_bounds__(TMA_THREADS, 2)
     k_iterate_tma(const Args<R, M::NSET> a, const __grid_constant__ TmaMaps T,
                   const PlaneAddr<typename St::T, M::Q> P, int R_rows, int* err, long long wait_cycles_arg,
@@ -392,7 +392,9 @@ __global__ void __launch_bounds__(TMA_THREADS, 2)
       yt -= rows_per_plane;
       z++;
     }
-    if (act) pair_update_store<M, R, St>(v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
+    if (act)
+      pair_update_store<M, R, St, PlaneAddr<typename St::T, M::Q>, Args<R, M::NSET>, LANES>(
+          v, (flag_t)(fl2 & 0xffffu), (flag_t)(fl2 >> 16), a, P, node);
   }
 }
 
