@@ -1130,10 +1130,12 @@ struct Pack16<StoreBF16<SH>> {
 // iterations (no Globals).
 // AR: Args<R, M::NSET>, or for the packed models a view with the same
 // members s[], k[], zone (SharedArgsView).
-// LANES (register pair kernels of models with identity rates, d3q19): a pair
-// where one node collides runs the other lane at the identity rates instead
-// of parking it. The tile-staged kernels keep parking: their 96-register cap
-// (18 warps per SM) spills the per-lane rates, which cost more than parking.
+// LANES (models with identity rates, d3q19): a pair where one node collides
+// runs the other lane at the identity rates instead of parking it. The
+// register pair kernels always do; the one-lattice tile-staged kernel does
+// when such pairs are at least 1% of the lattice (at its 96-register cap the
+// per-lane rates spill, which costs more than parking when they are rare);
+// the batch tile-staged kernel, with more state per warp, parks.
 template <class M, class R, class St, class A, class AR, bool LANES = false>
 __device__ __forceinline__ void pair_update_store(float2 (&v)[M::Q], flag_t fla, flag_t flb, const AR& a, const A& P,
                                                   unsigned node) {
