@@ -275,7 +275,8 @@ def aggregate_serving(reps, rep: dict, tts: list, updates: float, ideal_s: float
             "fraction_of_single": ideal / busy if busy else 0.0, "gpus": reps.world}
 
 
-def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150, reps=None) -> dict:
+def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150, reps=None,
+            solo_nodes=4_000_000) -> dict:
     """With reps over N > 1 ranks the requests are dealt out round-robin in
     arrival order (request i to rank i mod N), each rank serving its share on
     its own GPU with no exchange; the figures are aggregated over the ranks."""
@@ -285,7 +286,7 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150,
     out = {"config": f"5: serving, Poisson arrivals (rate {rate}/s, seed 0), 70% d2q9 obstacle channels (config-4 "
                      "sizes), 30% d3q19 porous boxes (edge U[64,256], p U[0.02,0.15]), iterations U[500,5000], "
                      f"admission by footprint under {budget_gb} GB (pools of 4 + 24 GiB set aside at start-up), resident "
-                     "lattices, continuous batching",
+                     f"lattices, continuous batching; requests of at least {solo_nodes} nodes as lattices of their own",
            "gpus": reps.world, "runs": {}}
     for st in storages:
         reqs = serve_requests(n_requests, rate)[reps.rank::reps.world]
@@ -293,7 +294,7 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150,
         # admissions then take memory like those of a running server instead of growing the pools
         srv = Server(("d2q9", "d3q19"), "fp32", st, budget_bytes=budget_gb << 30,
                      launch={"d2q9": (64, 64, 64), "d3q19": (64, 16, 16) if st == "same" else (64, 64, 16)},
-                     reserve={"d2q9": 4 << 30, "d3q19": 24 << 30})
+                     reserve={"d2q9": 4 << 30, "d3q19": 24 << 30}, solo_nodes=solo_nodes)
         reps.barrier()
         rep = srv.run(reqs)
         done = srv.done

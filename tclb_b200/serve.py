@@ -17,6 +17,14 @@ A request can be cancelled while it waits, while it is pending, or while it
 runs (it leaves at its batch's next boundary). Time to solution = completion
 time - arrival time.
 
+Optionally (`solo_nodes`), a request of at least that many nodes runs as a
+lattice of its own instead of joining its model's batch: one of the largest
+cases fills the GPU alone, and the one-lattice kernels carry none of the
+batch's per-tile case descriptors, so they run faster on it. It starts as soon
+as it is admitted, on its own stream, in chunks of `solo_iters` iterations
+whose completion is queried without blocking; its last iteration computes
+its Globals. Admission, the budget, cancellation and results are the same.
+
 No counterpart in the reference (TCLB runs one case per process).
 """
 from __future__ import annotations
@@ -30,6 +38,19 @@ import numpy as np
 
 from . import models as M
 from .batch import AdmissionRefused, Batch, CaseSpec, case_bytes
+
+
+@dataclass
+class _Solo:
+    """A request running as a lattice of its own."""
+
+    request: "Request"
+    lattice: object
+    stream: object
+    remaining: int
+    event: object = None  # completion of the chunk in flight
+    chunk: int = 0
+    cancel: bool = False
 
 
 @dataclass
@@ -120,7 +141,8 @@ class Server:
     def __init__(self, models=("d2q9", "d3q19"), precision="fp32", storage="same", budget_bytes: int = 150 << 30,
                  launch: Optional[Dict[str, Tuple[int, int, int]]] = None, max_cases: int = 4096,
                  high_priority: Tuple[str, ...] = ("d2q9",), max_bypass_s: float = 5.0,
-                 reserve: Optional[Dict[str, int]] = None):
+                 reserve: Optional[Dict[str, int]] = None, solo_nodes: Optional[int] = None,
+                 solo_iters: int = 64):
         """reserve: device bytes to set aside per model at start-up (Batch.reserve), so that the
         first admissions take memory from the pools like those of a server that has been running;
         the sum must stay within the budget."""
@@ -146,6 +168,8 @@ class Server:
         self.done: List[Request] = []
         self.cancelled: List[Request] = []
         self._cancel_resident: set = set()
+        self.solo_nodes, self.solo_iters = solo_nodes, int(solo_iters)
+        self.solo: Dict[int, _Solo] = {}  # rid -> a request running as its own lattice
         self.t0 = time.perf_counter()
         self.rounds = 0
         self.busy = 0.0  # seconds with GPU work in flight (step to sync)
@@ -183,6 +207,9 @@ class Server:
             if r.rid == rid and not r.cancelled:
                 self._cancel_resident.add((m, cid))
                 return True
+        if rid in self.solo and not self.solo[rid].cancel:
+            self.solo[rid].cancel = True  # leaves when its chunk in flight has finished
+            return True
         return False
 
     def _mark_cancelled(self, r: Request, release: bool = True):
@@ -197,7 +224,60 @@ class Server:
         model's pending list for the batch's next replay boundary."""
         for r in self.adm.admit(self.now()):
             r.admitted = self.now()
-            self.pending[r.model].append(r)
+            if self.solo_nodes is not None and r.nodes >= self.solo_nodes:
+                self._start_solo(r)
+            else:
+                self.pending[r.model].append(r)
+
+    def _start_solo(self, r: Request):
+        import torch
+
+        from .lattice import Lattice
+
+        nz, ny, nx = r.spec.shape
+        lat = Lattice(r.model, nx, ny, nz, precision=self.precision, storage=self.storage)
+        fl = r.spec.flags if r.spec.flags.ndim == 3 else r.spec.flags[None]
+        lat.set_flags(np.ascontiguousarray(fl, np.uint16))
+        for k, v in r.spec.settings.items():
+            lat.SetSetting(k, v)
+        for z, d in r.spec.zone_settings.items():
+            for k, v in d.items():
+                lat.set_zone_setting(k, v, z)
+        lat.Init()  # BaseInit equilibrium, as a batch case starts
+        self.solo[r.rid] = _Solo(r, lat, torch.cuda.Stream(), int(r.spec.niter))
+
+    def _step_solo(self, sl: _Solo) -> bool:
+        """Advance one request running as its own lattice; True if anything happened."""
+        r = sl.request
+        if sl.event is not None:
+            if not sl.event.query():
+                return False
+            sl.event = None
+            sl.remaining -= sl.chunk
+        if sl.cancel:
+            sl.lattice.close()
+            del self.solo[r.rid]
+            self._mark_cancelled(r)
+            return True
+        if sl.remaining <= 1:
+            if sl.remaining == 1:  # the last iteration integrates the Globals (returns when done)
+                sl.lattice.Iterate(1, M.ITER_NORM | M.ITER_LASTGLOB, stream=sl.stream.cuda_stream)
+            r.globals = sl.lattice.globals
+            if r.want_quantity:
+                r.quantity = sl.lattice.GetQuantity(r.want_quantity)
+            sl.lattice.close()
+            del self.solo[r.rid]
+            self.adm.release(r)
+            r.finished = self.now()
+            self.done.append(r)
+            return True
+        import torch
+
+        sl.chunk = min(sl.remaining - 1, self.solo_iters)
+        sl.lattice.Iterate(sl.chunk, M.ITER_NORM, stream=sl.stream.cuda_stream)
+        sl.event = torch.cuda.Event()
+        sl.event.record(sl.stream)
+        return True
 
     def _join(self, model):
         """At a replay boundary of the model's batch: its pending cases join."""
@@ -239,7 +319,8 @@ class Server:
         self.t0 = time.perf_counter()
         inflight = {m: False for m in self.batches}
         t_prev = time.perf_counter()
-        while (self.adm.waiting() or any(self.pending.values()) or self.resident) and self.now() < timeout_s:
+        while (self.adm.waiting() or any(self.pending.values()) or self.resident or self.solo) and \
+                self.now() < timeout_s:
             progressed = False
             while cancel_events and cancel_events[0][0] <= self.now():
                 self.cancel(cancel_events.pop(0)[1])
@@ -260,17 +341,21 @@ class Server:
                     inflight[m] = True
                     self.rounds += 1
                     progressed = True
+            for sl in list(self.solo.values()):
+                progressed = self._step_solo(sl) or progressed
             t = time.perf_counter()
-            if any(inflight.values()):
+            busy = {m: f or any(sl.event is not None and sl.request.model == m for sl in self.solo.values())
+                    for m, f in inflight.items()}
+            if any(busy.values()):
                 self.busy += t - t_prev  # GPU work was in flight during this interval
-                for m, f in inflight.items():
+                for m, f in busy.items():
                     if f:
                         self.busy_by_model[m] += t - t_prev
-                if all(inflight.values()):
+                if all(busy.values()):
                     self.busy_all += t - t_prev
             t_prev = t
             if not progressed:
-                if not any(inflight.values()):
+                if not any(inflight.values()) and not any(sl.event is not None for sl in self.solo.values()):
                     nxt = [q[0].arrival for q in self.adm.queues.values() if q]
                     dt = (min(nxt) - self.now()) if nxt else 0.0
                     if dt > 0:
@@ -290,8 +375,12 @@ class Server:
                 "p99_s": float(np.percentile(tts, 99)), "rounds": self.rounds, "cancelled": len(self.cancelled),
                 "busy_by_model_s": dict(self.busy_by_model), "busy_all_models_s": self.busy_all,
                 "updates_by_model": {m: sum(r.updates for r in self.done if r.model == m) for m in self.batches},
-                "pending": self.adm.waiting() + sum(len(v) for v in self.pending.values()) + len(self.resident)}
+                "pending": self.adm.waiting() + sum(len(v) for v in self.pending.values()) + len(self.resident) +
+                len(self.solo)}
 
     def close(self):
+        for sl in self.solo.values():
+            sl.lattice.close()
+        self.solo.clear()
         for b in self.batches.values():
             b.close()

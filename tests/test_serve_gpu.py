@@ -79,3 +79,34 @@ def test_cancel_waiting_pending_and_running_requests():
     alone.run([r2])
     alone.close()
     assert rel_l2(r.quantity, r2.quantity) <= 1e-6
+
+
+def test_large_requests_as_their_own_lattice():
+    """With solo_nodes, requests of at least that many nodes run as lattices of their
+    own (in chunks on their own streams) while the rest are batched: every result is
+    the one the batched path gives, and a large request cancelled while it runs
+    leaves with its memory returned."""
+    launch = {"d2q9": (64, 4, 16), "d3q19": (32, 8, 8)}
+    reqs = small_requests()  # d3q19 boxes of 32^3 and 64^3 nodes; 64^3 runs as its own lattice
+    budget = 4 << 30
+    solo = Server(("d2q9", "d3q19"), "fp32", "same", budget_bytes=budget, launch=launch, solo_nodes=64 ** 3,
+                  solo_iters=7)
+    rep = solo.run(reqs)
+    solo.close()
+    assert rep["requests"] == len(reqs) and rep["pending"] == 0 and solo.used == 0
+    ref = [Request(r.rid, r.model, r.spec, r.arrival, want_quantity="U") for r in small_requests()]
+    batched = Server(("d2q9", "d3q19"), "fp32", "same", budget_bytes=budget, launch=launch)
+    batched.run(ref)
+    batched.close()
+    for r, q in zip(reqs, ref):
+        assert rel_l2(r.quantity, q.quantity) <= 1e-6, r.rid
+        assert np.allclose(r.globals, q.globals, rtol=1e-9, atol=1e-15), r.rid
+    # cancel the large request while it runs
+    reqs = small_requests()
+    big = reqs[7]
+    big.spec = CaseSpec(big.spec.flags, big.spec.settings, big.spec.zone_settings, 200000)
+    srv = Server(("d2q9", "d3q19"), "fp32", "same", budget_bytes=budget, launch=launch, solo_nodes=64 ** 3)
+    rep = srv.run(reqs, cancels=[(0.2, 7)])
+    srv.close()
+    assert big.cancelled and big.globals is None
+    assert rep["requests"] == len(reqs) - 1 and rep["pending"] == 0 and srv.used == 0
