@@ -276,10 +276,16 @@ def aggregate_serving(reps, rep: dict, tts: list, updates: float, ideal_s: float
 
 
 def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150, reps=None,
-            solo_nodes=4_000_000) -> dict:
+            solo_nodes=None) -> dict:
     """With reps over N > 1 ranks the requests are dealt out round-robin in
     arrival order (request i to rank i mod N), each rank serving its share on
-    its own GPU with no exchange; the figures are aggregated over the ranks."""
+    its own GPU with no exchange; the figures are aggregated over the ranks.
+    solo_nodes: requests of at least that many nodes run as lattices of their own (a number, or a dict
+    by storage). Default: 10M nodes in FP32 storage, where batched and one-lattice kernels are both
+    close to the HBM roofline and only the largest boxes gain from running alone; 4M nodes in 16-bit
+    storage, where the batch's tile-staged kernel falls further behind the one-lattice kernels."""
+    if solo_nodes is None:
+        solo_nodes = {"same": 10_000_000, "fp16s": 4_000_000}
     from .replicas import Replicas
 
     reps = reps or Replicas("gloo")
@@ -294,7 +300,8 @@ def config5(n_requests=120, rate=6.0, storages=("same", "fp16s"), budget_gb=150,
         # admissions then take memory like those of a running server instead of growing the pools
         srv = Server(("d2q9", "d3q19"), "fp32", st, budget_bytes=budget_gb << 30,
                      launch={"d2q9": (64, 64, 64), "d3q19": (64, 16, 16) if st == "same" else (64, 64, 16)},
-                     reserve={"d2q9": 4 << 30, "d3q19": 24 << 30}, solo_nodes=solo_nodes)
+                     reserve={"d2q9": 4 << 30, "d3q19": 24 << 30},
+                     solo_nodes=solo_nodes.get(st) if isinstance(solo_nodes, dict) else solo_nodes)
         reps.barrier()
         rep = srv.run(reqs)
         done = srv.done
