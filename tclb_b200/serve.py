@@ -145,7 +145,9 @@ class Server:
                  solo_iters: int = 64):
         """reserve: device bytes to set aside per model at start-up (Batch.reserve), so that the
         first admissions take memory from the pools like those of a server that has been running;
-        the sum must stay within the budget."""
+        the sum must stay within the budget. The reserve does not count against the budget, and a
+        request run as a lattice of its own (solo_nodes) allocates its memory outside the pools
+        (its footprint does count), so budget + reserve must fit the device."""
         if reserve and sum(reserve.values()) > budget_bytes:
             raise ValueError("reserve exceeds the budget")
         self.precision, self.storage = precision, storage
