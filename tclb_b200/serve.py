@@ -343,11 +343,15 @@ class Server:
                     inflight[m] = True
                     self.rounds += 1
                     progressed = True
+            # a model with a lattice of its own in flight during this interval, including one whose
+            # chunk completes now and whose last (Globals) iteration runs in _step_solo, counts as busy
+            solo_busy = {sl.request.model for sl in self.solo.values() if sl.event is not None}
             for sl in list(self.solo.values()):
+                solo_busy |= {sl.request.model} if sl.remaining <= 1 or sl.event is not None else set()
                 progressed = self._step_solo(sl) or progressed
+            solo_busy |= {sl.request.model for sl in self.solo.values() if sl.event is not None}
             t = time.perf_counter()
-            busy = {m: f or any(sl.event is not None and sl.request.model == m for sl in self.solo.values())
-                    for m, f in inflight.items()}
+            busy = {m: f or m in solo_busy for m, f in inflight.items()}
             if any(busy.values()):
                 self.busy += t - t_prev  # GPU work was in flight during this interval
                 for m, f in busy.items():
