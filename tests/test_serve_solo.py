@@ -118,3 +118,9 @@ def test_cancel_leaves_after_the_chunk_in_flight(server):
     assert r.cancelled and r.globals is None and lat.closed
     assert server.cancelled == [r] and server.done == [] and server.adm.used == 0
     assert all(t == M.ITER_NORM for _, t in lat.calls)
+
+
+def test_reserve_above_the_budget_is_refused():
+    """The pools set aside at start-up must fit the budget; checked before any batch is made."""
+    with pytest.raises(ValueError):
+        Server(("d2q9", "d3q19"), budget_bytes=1 << 20, reserve={"d2q9": 1 << 19, "d3q19": 1 << 20})
